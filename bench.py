@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Voxelizer forward+backward throughput (Gvox-evals/s) on one B200.
+
+Workload (default ``mri128x128x96_n50k``): the 128x128x96 complex64 plain
+3DGSMR reconstruction at its initial state -- a synthetic 10-ellipsoid
+phantom with polynomial phase, 8 ring coils, R=6 variable-density mask with
+a 24x24 calibration region, 1e-3 complex noise, and 50,000 Gaussians seeded
+from the zero-filled image (random centres, 3-NN isotropic scale, identity
+rotation, density 0.2 x image).  One step = preprocess + tile binning +
+forward + backward of the voxelizer with a complex standard-normal upstream
+gradient.  Units: candidate Gaussian-voxel evaluations E (sum over 8^3 tiles
+of |list| x |voxels|) per second, forward+backward counted once.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``--impl reference`` times the CPU port of the reference's own CPU path
+(oracle/torch_port.py) on the host cores.  Under torchrun every rank runs
+an independent replica (the path has no cross-GPU exchange); rank 0 prints.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "mri128x128x96_n50k": dict(shape=(128, 128, 96), n=50_000, kind="from_image"),
+    "mri128x128x96_n500k": dict(shape=(128, 128, 96), n=500_000, kind="from_image"),
+    "cube64_n20k": dict(shape=(64, 64, 64), n=20_000, kind="random"),
+}
+TILE = 8
+# Algorithmic FP32-pipe operations per candidate evaluation (forward 15,
+# backward 33: recompute, cutoff test, density / centre / covariance terms).
+OPS_FWD, OPS_BWD = 15, 33
+SMS, LANES = 148, 128
+
+
+def make_inputs(name):
+    from gs_tmi_b200 import synthetic
+
+    wl = WORKLOADS[name]
+    if wl["kind"] == "from_image":
+        case = synthetic.mri_case(wl["shape"], n_coils=8, accel=6.0, calib=24, seed=0)
+        gs = synthetic.from_image_init(case.zero_filled, wl["n"], seed=0)
+    else:
+        gs = synthetic.random_gaussians(wl["n"], wl["shape"], seed=0)
+    return gs, synthetic.upstream_grad(wl["shape"], seed=1)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        mhz = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
+
+
+def count_library_launches(fn, dev):
+    """Kernels one call of `fn` launches, read from the CUDA activity trace."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        torch.cuda.synchronize(dev)
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize(dev)
+        names = [e.name for e in prof.events() if e.device_type.name == "CUDA" and "Memset" not in e.name
+                 and "Memcpy" not in e.name]
+        return len(names), sorted(set(names))
+    except Exception as exc:  # profiler unavailable: report unknown
+        return None, [f"profiler unavailable: {exc}"]
+
+
+def cpu_baseline(gs, gv, shape, seconds=12.0):
+    """CPU port of the reference's CPU path on a bounded random sample of
+    tiles of the same workload, all host threads."""
+    from oracle import oracle as O
+    from oracle import torch_port
+
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    p = tuple(t.numpy() for t in gs.tensors())
+    c, r, _ = O.preprocess_f32(*p[:3], shape)
+    tr, pid = O.build_tile_pairs(c, r, shape, TILE)
+    d, h, w = shape
+    nt = tr.shape[0]
+    order = np.random.default_rng(0).permutation(nt)
+    per_tile = (tr[:, 1] - tr[:, 0]).astype(np.int64) * TILE ** 3  # interior tiles (shape divisible by 8)
+    torch_port.time_fwd_bwd(p, shape, TILE, tr, pid, gv.numpy(), order[:2])  # warm-up
+    done, evals, t_total, chunk = 0, 0, 0.0, 8
+    while t_total < seconds and done < nt:
+        tiles = order[done:done + chunk]
+        t_total += torch_port.time_fwd_bwd(p, shape, TILE, tr, pid, gv.numpy(), tiles)
+        evals += int(per_tile[tiles].sum())
+        done += len(tiles)
+        chunk = min(chunk * 2, 64)
+    return {"value": evals / t_total / 1e9, "unit": "Gvox-evals/s", "cores": torch.get_num_threads(),
+            "kind": "port", "seconds": t_total,
+            "sample": f"{done} of {nt} tiles (random, seed 0) of the same workload, {evals} evals, "
+                      f"{t_total:.1f} s, torch {torch.__version__} FP32 on host cores"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    name = args.workload
+    gs, gv = make_inputs(name)
+    shape = WORKLOADS[name]["shape"]
+    vals, times = [], []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(gs, gv, shape, seconds=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+        if i >= args.warmup:
+            vals.append(b["value"])
+            times.append(b["seconds"])
+    v = statistics.mean(vals)
+    out = {"metric": "fwd+bwd Gvox-evals/s", "value": v, "unit": "Gvox-evals/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": name, "volume": list(shape), "gaussians": WORKLOADS[name]["n"],
+                      "tile_size": TILE, "parallelism": "replicas"},
+           "cpu_baseline": dict(b, value=v),
+           "e2e": {"value": v, "unit": "Gvox-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, world, dist):
+    from gs_tmi_b200 import TileVoxelizer
+    from gs_tmi_b200._lib import GSV_BACKWARD_DETERMINISTIC, GsvGrads, GsvParams, check, lib
+    from gs_tmi_b200.tile_voxelizer import _ptr, _shape, _stream, prepare_and_bin
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    name = args.workload
+    shape = WORKLOADS[name]["shape"]
+    gs, gv = make_inputs(name)
+    n = gs.n
+    flags = GSV_BACKWARD_DETERMINISTIC if args.deterministic else 0
+    params = tuple(t.to(dev).contiguous() for t in gs.tensors())
+    gvd = gv.to(dev).contiguous()
+    gshape = _shape(shape, TILE)
+    plan = prepare_and_bin(params, gshape, flags)  # sizes the pair workspace (one sync, untimed)
+    cap, total = plan.capacity, plan.total
+    tr_host = None
+    outs = [torch.empty_like(t) for t in params]
+    vol = torch.empty(shape, dtype=torch.complex64, device=dev)
+    gp = GsvParams(*(t.data_ptr() for t in params), n)
+    gg = GsvGrads(*(o.data_ptr() for o in outs))
+    st = _stream(dev)
+    wsg, wsp = _ptr(plan.ws_gauss), _ptr(plan.ws_pairs)
+
+    def prep_bin():
+        check(lib.gsv_prepare(ctypes.byref(gp), gshape, wsg, plan.gauss_bytes, None, st), "prepare")
+        check(lib.gsv_bin(gshape, n, wsg, wsp, plan.pair_bytes, cap, st), "bin")
+
+    def fwd():
+        check(lib.gsv_forward(gshape, n, wsg, wsp, cap, _ptr(vol), st), "forward")
+
+    def bwd():
+        check(lib.gsv_backward(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags, st),
+              "backward")
+
+    def step():
+        prep_bin()
+        fwd()
+        bwd()
+
+    # E from the executed binning
+    tr_ptr, _ = plan.views()
+    ntiles = lib.gsv_num_tiles(gshape)
+    off = tr_ptr - plan.ws_gauss.data_ptr()
+    tr_host = plan.ws_gauss[off:off + 8 * ntiles].view(torch.int32).reshape(-1, 2).cpu().numpy()
+    d, h, w = shape
+    nvox = []
+    for t in range(ntiles):
+        td, rem = divmod(t, (-(-h // TILE)) * (-(-w // TILE)))
+        th, tw = divmod(rem, -(-w // TILE))
+        nvox.append(min(TILE, d - td * TILE) * min(TILE, h - th * TILE) * min(TILE, w - tw * TILE))
+    evals = int(((tr_host[:, 1] - tr_host[:, 0]).astype(np.int64) * np.array(nvox)).sum())
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    n_launch, kernel_names = count_library_launches(step, dev)
+
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    cur = torch.cuda.current_stream(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(cur)
+            prep_bin()
+            ev[i][1].record(cur)
+            fwd()
+            ev[i][2].record(cur)
+            bwd()
+            ev[i][3].record(cur)
+        torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    t_step = [ev[i][0].elapsed_time(ev[i][3]) for i in range(args.steps)]
+    t_bin = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
+    t_fwd = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
+    t_bwd = [ev[i][2].elapsed_time(ev[i][3]) for i in range(args.steps)]
+    total_ms = sum(t_step)
+    _, fl = plan.read_status(st)
+    if fl:
+        raise RuntimeError(f"voxelizer status flags {fl} during the timed region")
+
+    # e2e through the public module with pinned host buffers
+    vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic)
+    host_in = [t.pin_memory() for t in gs.tensors()]
+    gv_host = gv.pin_memory()
+    host_out = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in gs.tensors()]
+    vol_host = torch.empty(shape, dtype=torch.complex64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host_in) + gv_host.numel() * 8
+    d2h = sum(t.numel() * t.element_size() for t in host_out) + vol_host.numel() * 8
+
+    def e2e_step():
+        ps = [t.to(dev, non_blocking=True).requires_grad_(True) for t in host_in]
+        g = gv_host.to(dev, non_blocking=True)
+        v = vox(ps[0], ps[1], ps[2], torch.complex(ps[3], ps[4]))
+        v.backward(g)
+        vol_host.copy_(v.detach(), non_blocking=True)
+        for o, p in zip(host_out, ps):
+            o.copy_(p.grad, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    e0.record(cur)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(cur)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+
+    stats = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = stats.tolist()
+    if rank != 0:
+        return
+    pk, pk_kind = peaks()
+    clocks = clk.summary()
+    sm_mhz = float(pk.get("sm_max_mhz", 1965.0))
+    peak_ops = SMS * LANES * sm_mhz * 1e6
+    bwd_ms = statistics.mean(t_bwd)
+    fwd_ms = statistics.mean(t_fwd)
+    ach_bwd = evals * OPS_BWD / (bwd_ms * 1e-3)
+    ach_fwd = evals * OPS_FWD / (fwd_ms * 1e-3)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(name, {}).get("k_backward8")
+    vol_bytes = 2 * 8 * d * h * w  # write the volume, read its gradient
+    value = evals * args.steps * world / (total_ms * 1e-3) / 1e9
+    out = {
+        "metric": "fwd+bwd Gvox-evals/s", "value": value, "unit": "Gvox-evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": name, "volume": list(shape), "gaussians": n, "tile_size": TILE, "pairs": total,
+                   "evals_per_step": evals, "deterministic": bool(args.deterministic),
+                   "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
+        "breakdown_ms": {"prepare_bin": statistics.mean(t_bin), "forward": fwd_ms, "backward": bwd_ms},
+        "roofline": {"bound": "fp32_issue", "kernel": "gsv_backward (k_backward8 + k_finalize)",
+                     "achieved": ach_bwd / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s",
+                     "frac": ach_bwd / peak_ops, "traffic": traffic,
+                     "ops_per_eval": OPS_BWD,
+                     "peak_source": f"{SMS} SMs x {LANES} FP32 lanes x sm_max_mhz {sm_mhz:.0f} ({pk_kind} peaks)",
+                     "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
+                     "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9,
+                             "peak_gbs": pk.get("hbm_gbs")}},
+        "e2e": {"value": evals * args.steps * world / (e2e_ms * 1e-3) / 1e9, "unit": "Gvox-evals/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
+                "api": "gs_tmi_b200.TileVoxelizer forward + autograd backward"},
+        "gpu_launches": None if n_launch is None else n_launch * args.steps,
+        "launches_per_step": n_launch, "kernels": kernel_names,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(gs, gv, shape)
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mri128x128x96_n50k")
+    ap.add_argument("--deterministic", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

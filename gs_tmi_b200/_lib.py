@@ -1,0 +1,97 @@
+"""ctypes binding of ``lib/libgsv_b200.so`` (the C ABI of ``include/gsv.h``).
+
+There is deliberately no fallback: if the sm_100a library is missing the
+import of this module raises, and every voxelizer entry point with it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgsv_b200.so")
+
+GSV_OK = 0
+GSV_ERR_INVALID_ARGUMENT = 1
+GSV_ERR_CAPACITY = 2
+GSV_ERR_CUDA = 3
+GSV_ERR_EMPTY_BOX = 4
+GSV_ERR_TOO_MANY_PAIRS = 5
+
+GSV_FLAG_CAPACITY_OVERFLOW = 0x1
+GSV_FLAG_EMPTY_BOX = 0x2
+GSV_FLAG_TOO_MANY_PAIRS = 0x4
+
+GSV_BACKWARD_DETERMINISTIC = 0x1
+
+
+class GsvShape(ctypes.Structure):
+    _fields_ = [("d", ctypes.c_int32), ("h", ctypes.c_int32), ("w", ctypes.c_int32),
+                ("tile_size", ctypes.c_int32)]
+
+
+class GsvParams(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("scales", ctypes.c_void_p),
+                ("rotations", ctypes.c_void_p), ("density_r", ctypes.c_void_p),
+                ("density_i", ctypes.c_void_p), ("n", ctypes.c_int64)]
+
+
+class GsvGrads(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("scales", ctypes.c_void_p),
+                ("rotations", ctypes.c_void_p), ("density_r", ctypes.c_void_p),
+                ("density_i", ctypes.c_void_p)]
+
+
+# name -> (restype, argtypes); the complete exported C ABI.
+_vp, _i32, _i64, _sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_S, _P, _G = GsvShape, ctypes.POINTER(GsvParams), ctypes.POINTER(GsvGrads)
+SIGNATURES = {
+    "gsv_abi_version": (ctypes.c_int, []),
+    "gsv_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "gsv_last_error": (ctypes.c_char_p, []),
+    "gsv_num_tiles": (_i64, [_S]),
+    "gsv_gauss_workspace_bytes": (_sz, [_i64, _S]),
+    "gsv_pair_workspace_bytes": (_sz, [_i64, _S, ctypes.c_int]),
+    "gsv_prepare": (ctypes.c_int, [_P, _S, _vp, _sz, _i64p, _vp]),
+    "gsv_bin": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp]),
+    "gsv_bin_views": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "gsv_read_status": (ctypes.c_int, [_S, _i64, _vp, _i64p, _i32p, _vp]),
+    "gsv_forward": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, _vp, _vp]),
+    "gsv_backward": (ctypes.c_int, [_P, _S, _vp, _vp, _i64, _vp, _G, ctypes.c_int, _vp]),
+    "gsv_build_tile_pairs_count": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _sz, _i64p, _vp]),
+    "gsv_build_tile_pairs_fill": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp, _vp, _vp]),
+    "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
+    "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the sm_100a voxelizer library with "
+            "`python -m gs_tmi_b200.build` (this package has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+class GsvError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib.gsv_status_string(status).decode()
+        if status == GSV_ERR_CUDA:
+            msg += ": " + lib.gsv_last_error().decode()
+        super().__init__(f"{where}: {msg}")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != GSV_OK:
+        raise GsvError(status, where)

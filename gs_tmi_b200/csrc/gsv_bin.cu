@@ -1,0 +1,483 @@
+// gsv_bin.cu -- preprocess and tile binning (device radix sort), sm_100a.
+//
+// Binning is bit-exact with build_tile_pairs (3DGS/3dgsVC/gaussian/
+// tile_voxelizer.py:87-162): the FP32 center/radius follow :284-286 op for
+// op, the voxel box uses floor/ceil + clamp (:97-105), the tile box integer
+// division + clamp (:107-114), pairs are generated Gaussian-major in
+// (d,h,w) raster order (:126-145) and stably sorted by tile id, so each
+// tile's list is in ascending Gaussian id; empty tiles keep range (0,0)
+// (:151-161).  Unlike the reference there is no host synchronisation unless
+// the caller asks for the pair total.
+#include <cub/cub.cuh>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "gsv_common.cuh"
+
+using namespace gsv;
+
+namespace {
+
+thread_local char g_last_error[512] = {0};
+
+constexpr int kMaxTilesPerAxis = 65535;  // box packing: 16 bits per field
+
+struct ShapeInfo {
+    int32_t d, h, w, ts, ntd, nth, ntw;
+    int64_t ntiles;
+    bool ok;
+};
+
+ShapeInfo shape_info(gsv_shape s) {
+    ShapeInfo r{};
+    r.ok = s.d > 0 && s.h > 0 && s.w > 0 && s.tile_size > 0 && s.d < (1 << 24) && s.h < (1 << 24) &&
+           s.w < (1 << 24);
+    if (!r.ok) return r;
+    r.d = s.d; r.h = s.h; r.w = s.w; r.ts = s.tile_size;
+    r.ntd = (s.d + s.tile_size - 1) / s.tile_size;
+    r.nth = (s.h + s.tile_size - 1) / s.tile_size;
+    r.ntw = (s.w + s.tile_size - 1) / s.tile_size;
+    r.ok = r.ntd <= kMaxTilesPerAxis && r.nth <= kMaxTilesPerAxis && r.ntw <= kMaxTilesPerAxis;
+    r.ntiles = int64_t(r.ntd) * r.nth * r.ntw;
+    r.ok = r.ok && r.ntiles < (int64_t(1) << 30);
+    return r;
+}
+
+int sort_end_bit(int64_t ntiles) {
+    // keys are tile ids in [0, ntiles]; ntiles is the padding sentinel.
+    int bits = 1;
+    while ((int64_t(1) << bits) <= ntiles) ++bits;
+    return bits;
+}
+
+GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
+    GaussLayout L{};
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int64_t*)nullptr, (int64_t*)nullptr,
+                                  int(n + 1));
+    L.scan_tmp_bytes = scan_bytes;
+    size_t o = 0;
+    L.rec = o;      o = align_up(o + size_t(n) * sizeof(Rec));
+    L.box = o;      o = align_up(o + size_t(n) * sizeof(int4));
+    L.counts = o;   o = align_up(o + size_t(n + 1) * sizeof(int64_t));
+    L.offsets = o;  o = align_up(o + size_t(n + 1) * sizeof(int64_t));
+    L.scan_tmp = o; o = align_up(o + scan_bytes);
+    L.ranges = o;   o = align_up(o + size_t(si.ntiles) * sizeof(int2));
+    L.accum = o;    o = align_up(o + size_t(n) * kMomStride * sizeof(float));
+    L.status = o;   o = align_up(o + sizeof(Status));
+    L.total = o;
+    return L;
+}
+
+PairLayout pair_layout(int64_t cap, const ShapeInfo& si, int flags) {
+    PairLayout L{};
+    size_t sort_bytes = 0;
+    const int end_bit = sort_end_bit(si.ntiles);
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const int32_t*)nullptr, (int32_t*)nullptr,
+                                    (const int32_t*)nullptr, (int32_t*)nullptr, int(cap > 0 ? cap : 1),
+                                    0, end_bit);
+    L.sort_tmp_bytes = sort_bytes;
+    size_t o = 0;
+    const size_t c = size_t(cap > 0 ? cap : 1);
+    L.keys_in = o;  o = align_up(o + c * sizeof(int32_t));
+    L.vals_in = o;  o = align_up(o + c * sizeof(int32_t));
+    L.keys_out = o; o = align_up(o + c * sizeof(int32_t));
+    L.vals_out = o; o = align_up(o + c * sizeof(int32_t));
+    L.sort_tmp = o; o = align_up(o + sort_bytes);
+    L.partials = o;
+    if (flags & GSV_BACKWARD_DETERMINISTIC) o = align_up(o + c * kMomStride * sizeof(float));
+    L.total = o;
+    return L;
+}
+
+template <typename T>
+T* at(void* base, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+}
+template <typename T>
+const T* at(const void* base, size_t off) {
+    return reinterpret_cast<const T*>(static_cast<const char*>(base) + off);
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+struct DevShape {
+    int32_t size[3];
+    int32_t nt[3];
+    int32_t ts;
+    float shape_f[3];
+    float hs[3];
+    float ih[3];
+};
+
+DevShape dev_shape(const ShapeInfo& si) {
+    DevShape s{};
+    s.size[0] = si.d; s.size[1] = si.h; s.size[2] = si.w;
+    s.nt[0] = si.ntd; s.nt[1] = si.nth; s.nt[2] = si.ntw;
+    s.ts = si.ts;
+    for (int a = 0; a < 3; ++a) {
+        s.shape_f[a] = float(s.size[a]);
+        s.hs[a] = s.shape_f[a] * 0.5f;
+        s.ih[a] = 1.0f / s.hs[a];  // host IEEE division, same as the device __fdiv_rn
+    }
+    return s;
+}
+
+// Tile box of one Gaussian; returns the tile count (<= 0 for an empty box).
+__device__ __forceinline__ int64_t tile_box(const DevShape& s, const float c[3], float r, int4* box) {
+    int32_t tlo[3], na[3];
+    int64_t cnt = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // (center_vox - r3).floor().int() / (center_vox + r3).ceil().int(), clamp (:97-105)
+        int32_t lo = __float2int_rz(floorf(__fsub_rn(c[a], r)));
+        int32_t hi = __float2int_rz(ceilf(__fadd_rn(c[a], r)));
+        lo = min(max(lo, 0), s.size[a] - 1);
+        hi = min(max(hi, 0), s.size[a] - 1);
+        // // tile_size, clamp (:107-114); lo, hi >= 0 here so C division == floor division
+        int32_t t0 = min(max(lo / s.ts, 0), s.nt[a] - 1);
+        int32_t t1 = min(max(hi / s.ts, 0), s.nt[a] - 1);
+        tlo[a] = t0;
+        na[a] = t1 - t0 + 1;
+        if (na[a] <= 0) cnt = 0;
+        else cnt *= na[a];
+    }
+    box->x = tlo[0] | (tlo[1] << 16);
+    box->y = tlo[2] | (max(na[0], 0) << 16);
+    box->z = max(na[1], 0) | (max(na[2], 0) << 16);
+    box->w = int32_t(cnt);
+    return cnt;
+}
+
+__global__ void __launch_bounds__(256) k_prepare(const float* __restrict__ pos,
+                                                 const float* __restrict__ scl,
+                                                 const float* __restrict__ rot,
+                                                 const float* __restrict__ dr,
+                                                 const float* __restrict__ di, int64_t n, DevShape s,
+                                                 Rec* __restrict__ recs, int4* __restrict__ boxes,
+                                                 int64_t* __restrict__ counts, Status* status) {
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g == 0) counts[n] = 0;
+    if (g >= n) return;
+    float p[3], sc[3], q[4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        p[a] = pos[g * 3 + a];
+        sc[a] = scl[g * 3 + a];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = rot[g * 4 + k];
+    float c[3], sv[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // center_vox = (positions + 1.0) * 0.5 * shape - 0.5   (:284)
+        c[a] = __fsub_rn(__fmul_rn(__fmul_rn(__fadd_rn(p[a], 1.0f), 0.5f), s.shape_f[a]), 0.5f);
+        sv[a] = __fmul_rn(sc[a], s.hs[a]);  // scale_vox (:285)
+    }
+    const float r = __fmul_rn(nanmax3(sv[0], sv[1], sv[2]), 3.0f);  // radius_vox (:286)
+    float qc[6];
+    qcoef_from_params(sc, q, s.ih, qc);
+    Rec R;
+    R.c0 = c[0]; R.c1 = c[1]; R.c2 = c[2];
+    R.q00 = qc[0]; R.q01x2 = qc[1]; R.q02x2 = qc[2]; R.q11 = qc[3]; R.q12x2 = qc[4]; R.q22 = qc[5];
+    R.rho_r = dr[g]; R.rho_i = di[g]; R.pad = 0.0f;
+    recs[g] = R;
+    int4 box;
+    int64_t cnt = tile_box(s, c, r, &box);
+    if (cnt <= 0) {
+        atomicOr(&status->flags, GSV_FLAG_EMPTY_BOX);
+        cnt = 0;
+        box.w = 0;
+    }
+    boxes[g] = box;
+    counts[g] = cnt;
+}
+
+__global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ center,
+                                                      const float* __restrict__ radius, int64_t n,
+                                                      DevShape s, int4* __restrict__ boxes,
+                                                      int64_t* __restrict__ counts, Status* status) {
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g == 0) counts[n] = 0;
+    if (g >= n) return;
+    float c[3] = {center[g * 3], center[g * 3 + 1], center[g * 3 + 2]};
+    int4 box;
+    int64_t cnt = tile_box(s, c, radius[g], &box);
+    if (cnt <= 0) {
+        atomicOr(&status->flags, GSV_FLAG_EMPTY_BOX);
+        cnt = 0;
+        box.w = 0;
+    }
+    boxes[g] = box;
+    counts[g] = cnt;
+}
+
+// One thread per Gaussian writes its (tile, gid) pairs in raster order.
+__global__ void __launch_bounds__(128) k_emit(const int4* __restrict__ boxes,
+                                              const int64_t* __restrict__ offsets, int64_t n,
+                                              DevShape s, int64_t cap, int32_t* __restrict__ keys,
+                                              int32_t* __restrict__ vals, Status* status) {
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g == 0) {
+        const int64_t total = offsets[n];
+        if (total > cap) atomicOr(&status->flags, GSV_FLAG_CAPACITY_OVERFLOW);
+        if (total > int64_t(INT32_MAX)) atomicOr(&status->flags, GSV_FLAG_TOO_MANY_PAIRS);
+    }
+    if (g >= n) return;
+    const int4 b = boxes[g];
+    const int32_t cnt = b.w;
+    if (cnt <= 0) return;
+    const int32_t t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
+    const int32_t n0 = (b.y >> 16) & 0xffff, n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
+    (void)n0;
+    int64_t o = offsets[g];
+    const int32_t gid = int32_t(g);
+    for (int32_t i = 0, j = 0, k = 0, c = 0; c < cnt; ++c) {
+        if (o >= cap) break;
+        const int32_t tile = ((t0 + i) * s.nt[1] + (t1 + j)) * s.nt[2] + (t2 + k);
+        keys[o] = tile;
+        vals[o] = gid;
+        ++o;
+        if (++k == n2) {
+            k = 0;
+            if (++j == n1) {
+                j = 0;
+                ++i;
+            }
+        }
+    }
+}
+
+__global__ void k_fill_sentinel(const int64_t* __restrict__ offsets, int64_t n, int64_t cap,
+                                int32_t sentinel, int32_t* __restrict__ keys,
+                                int32_t* __restrict__ vals) {
+    const int64_t total = offsets[n];
+    for (int64_t i = total + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cap;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        keys[i] = sentinel;
+        vals[i] = 0;
+    }
+}
+
+// Tile ranges from the sorted keys; empty tiles stay (0,0).
+__global__ void k_ranges(const int32_t* __restrict__ keys, const int64_t* __restrict__ offsets,
+                         int64_t n, int64_t cap, int64_t ntiles, int2* __restrict__ ranges) {
+    const int64_t total = min(offsets[n], cap);
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int32_t key = keys[i];
+    if (key < 0 || key >= ntiles) return;
+    if (i == 0 || keys[i - 1] != key) ranges[key].x = int32_t(i);
+    if (i == total - 1 || keys[i + 1] != key) ranges[key].y = int32_t(i + 1);
+}
+
+int grid_for(int64_t items, int block) {
+    int64_t g = (items + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > (int64_t(1) << 30)) g = int64_t(1) << 30;
+    return int(g);
+}
+
+int sync_total(const GaussLayout& L, void* ws, int64_t n, int64_t* total_host, cudaStream_t st) {
+    int64_t total = 0;
+    GSV_CUDA_TRY(cudaMemcpyAsync(&total, at<int64_t>(ws, L.offsets) + n, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st));
+    GSV_CUDA_TRY(cudaStreamSynchronize(st));
+    *total_host = total;
+    return GSV_OK;
+}
+
+// Shared tail of both binning flavours: emit, sort, ranges.
+int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+               int64_t cap, int32_t* vals_out_override, cudaStream_t st) {
+    if (cap < 0 || cap > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    const GaussLayout G = gauss_layout(n, si);
+    const PairLayout P = pair_layout(cap, si, 0);
+    if (ws_pairs_bytes < P.total || !ws_pairs) return GSV_ERR_INVALID_ARGUMENT;
+    DevShape s = dev_shape(si);
+    Status* status = at<Status>(ws_gauss, G.status);
+    const int64_t* offsets = at<int64_t>(ws_gauss, G.offsets);
+    int32_t* keys_in = at<int32_t>(ws_pairs, P.keys_in);
+    int32_t* vals_in = at<int32_t>(ws_pairs, P.vals_in);
+    int32_t* keys_out = at<int32_t>(ws_pairs, P.keys_out);
+    int32_t* vals_out = vals_out_override ? vals_out_override : at<int32_t>(ws_pairs, P.vals_out);
+    int2* ranges = at<int2>(ws_gauss, G.ranges);
+    GSV_CUDA_TRY(cudaMemsetAsync(ranges, 0, size_t(si.ntiles) * sizeof(int2), st));
+    if (cap == 0) return GSV_OK;
+    k_emit<<<grid_for(n, 128), 128, 0, st>>>(at<int4>(ws_gauss, G.box), offsets, n, s, cap, keys_in,
+                                             vals_in, status);
+    GSV_LAUNCH_CHECK();
+    k_fill_sentinel<<<grid_for(cap, 256) < 1184 ? grid_for(cap, 256) : 1184, 256, 0, st>>>(
+        offsets, n, cap, int32_t(si.ntiles), keys_in, vals_in);
+    GSV_LAUNCH_CHECK();
+    size_t sort_bytes = P.sort_tmp_bytes;
+    GSV_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at<void>(ws_pairs, P.sort_tmp), sort_bytes, keys_in,
+                                                 keys_out, vals_in, vals_out, int(cap), 0,
+                                                 sort_end_bit(si.ntiles), st));
+    k_ranges<<<grid_for(cap, 256), 256, 0, st>>>(keys_out, offsets, n, cap, si.ntiles, ranges);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C entry points
+// ---------------------------------------------------------------------------
+
+void gsv_detail_set_error(cudaError_t e, const char* what, const char* file, int line) {
+    snprintf(g_last_error, sizeof(g_last_error), "%s (%s) at %s:%d: %s", cudaGetErrorName(e), what,
+             file, line, cudaGetErrorString(e));
+}
+
+extern "C" {
+
+const char* gsv_last_error(void) { return g_last_error; }
+
+int gsv_abi_version(void) { return GSV_ABI_VERSION; }
+
+const char* gsv_status_string(int status) {
+    switch (status) {
+        case GSV_OK: return "ok";
+        case GSV_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case GSV_ERR_CAPACITY: return "pair capacity exceeded";
+        case GSV_ERR_CUDA: return "CUDA error";
+        case GSV_ERR_EMPTY_BOX: return "empty tile box (negative radius)";
+        case GSV_ERR_TOO_MANY_PAIRS: return "more than INT32_MAX tile pairs";
+        default: return "unknown status";
+    }
+}
+
+int64_t gsv_num_tiles(gsv_shape shape) {
+    ShapeInfo si = shape_info(shape);
+    return si.ok ? si.ntiles : -1;
+}
+
+size_t gsv_gauss_workspace_bytes(int64_t n, gsv_shape shape) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || n >= int64_t(INT32_MAX)) return 0;
+    return gauss_layout(n, si).total;
+}
+
+size_t gsv_pair_workspace_bytes(int64_t capacity, gsv_shape shape, int flags) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || capacity < 0 || capacity > int64_t(INT32_MAX)) return 0;
+    return pair_layout(capacity, si, flags).total;
+}
+
+int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
+                int64_t* total_pairs_host, void* stream) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || !p || p->n < 0 || p->n >= int64_t(INT32_MAX) || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
+    const int64_t n = p->n;
+    if (n > 0 && (!p->positions || !p->scales || !p->rotations || !p->density_r || !p->density_i))
+        return GSV_ERR_INVALID_ARGUMENT;
+    const GaussLayout L = gauss_layout(n, si);
+    if (ws_gauss_bytes < L.total) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Status* status = at<Status>(ws_gauss, L.status);
+    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(Status), st));
+    k_prepare<<<grid_for(n + 1, 256), 256, 0, st>>>(p->positions, p->scales, p->rotations, p->density_r,
+                                                    p->density_i, n, dev_shape(si), at<Rec>(ws_gauss, L.rec),
+                                                    at<int4>(ws_gauss, L.box), at<int64_t>(ws_gauss, L.counts),
+                                                    status);
+    GSV_LAUNCH_CHECK();
+    size_t scan_bytes = L.scan_tmp_bytes;
+    GSV_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at<void>(ws_gauss, L.scan_tmp), scan_bytes,
+                                               at<int64_t>(ws_gauss, L.counts),
+                                               at<int64_t>(ws_gauss, L.offsets), int(n + 1), st));
+    if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
+    return GSV_OK;
+}
+
+int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+            int64_t capacity, void* stream) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
+    return bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, nullptr,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int gsv_bin_views(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, int64_t capacity,
+                  int32_t** tile_ranges, int32_t** pair_ids) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || !ws_gauss || !ws_pairs) return GSV_ERR_INVALID_ARGUMENT;
+    if (tile_ranges) *tile_ranges = at<int32_t>(ws_gauss, gauss_layout(n, si).ranges);
+    if (pair_ids) *pair_ids = at<int32_t>(ws_pairs, pair_layout(capacity, si, 0).vals_out);
+    return GSV_OK;
+}
+
+int gsv_read_status(gsv_shape shape, int64_t n, const void* ws_gauss, int64_t* total_pairs,
+                    int32_t* flags, void* stream) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
+    const GaussLayout L = gauss_layout(n, si);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int64_t total = 0;
+    Status s{};
+    GSV_CUDA_TRY(cudaMemcpyAsync(&total, at<int64_t>(ws_gauss, L.offsets) + n, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st));
+    GSV_CUDA_TRY(cudaMemcpyAsync(&s, at<Status>(ws_gauss, L.status), sizeof(Status),
+                                 cudaMemcpyDeviceToHost, st));
+    GSV_CUDA_TRY(cudaStreamSynchronize(st));
+    if (total_pairs) *total_pairs = total;
+    if (flags) *flags = s.flags;
+    return GSV_OK;
+}
+
+int gsv_build_tile_pairs_count(const float* center_vox, const float* radius_vox, int64_t n,
+                               gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
+                               int64_t* total_pairs_host, void* stream) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || n >= int64_t(INT32_MAX) || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
+    if (n > 0 && (!center_vox || !radius_vox)) return GSV_ERR_INVALID_ARGUMENT;
+    const GaussLayout L = gauss_layout(n, si);
+    if (ws_gauss_bytes < L.total) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Status* status = at<Status>(ws_gauss, L.status);
+    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(Status), st));
+    k_count_compat<<<grid_for(n + 1, 256), 256, 0, st>>>(center_vox, radius_vox, n, dev_shape(si),
+                                                         at<int4>(ws_gauss, L.box),
+                                                         at<int64_t>(ws_gauss, L.counts), status);
+    GSV_LAUNCH_CHECK();
+    size_t scan_bytes = L.scan_tmp_bytes;
+    GSV_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at<void>(ws_gauss, L.scan_tmp), scan_bytes,
+                                               at<int64_t>(ws_gauss, L.counts),
+                                               at<int64_t>(ws_gauss, L.offsets), int(n + 1), st));
+    if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
+    return GSV_OK;
+}
+
+int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs,
+                              size_t ws_pairs_bytes, int64_t capacity, int32_t* tile_ranges,
+                              int32_t* pair_ids, void* stream) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || !ws_gauss || !tile_ranges || (capacity > 0 && !pair_ids))
+        return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, pair_ids, st);
+    if (rc != GSV_OK) return rc;
+    const GaussLayout L = gauss_layout(n, si);
+    GSV_CUDA_TRY(cudaMemcpyAsync(tile_ranges, at<int2>(ws_gauss, L.ranges), size_t(si.ntiles) * sizeof(int2),
+                                 cudaMemcpyDeviceToDevice, st));
+    return GSV_OK;
+}
+
+}  // extern "C"
+
+// Internal accessors for the render translation unit.
+namespace gsv {
+int layout_for(gsv_shape shape, int64_t n, int64_t cap, int flags, GaussLayout* G, PairLayout* P,
+               int64_t* ntiles) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0) return GSV_ERR_INVALID_ARGUMENT;
+    if (G) *G = gauss_layout(n, si);
+    if (P) *P = pair_layout(cap, si, flags);
+    if (ntiles) *ntiles = si.ntiles;
+    return GSV_OK;
+}
+}  // namespace gsv

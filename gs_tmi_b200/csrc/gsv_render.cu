@@ -1,0 +1,859 @@
+// gsv_render.cu -- forward / backward tile kernels and the gradient finalize.
+//
+// Work decomposition (tile edge 8, the reference default):
+//   one CTA of 4 warps per tile; every warp covers the whole 8x8x8 tile
+//   (lane l owns the two 8-voxel rows (d0+l/8, h0+l%8) and (d0+4+l/8, h0+l%8))
+//   and the tile's Gaussian list is split between the warps in chunks of 32.
+//   A warp stages its 32 Gaussians in shared memory, then walks them; for
+//   each Gaussian a lane evaluates its 16 voxels with the row form
+//   m = fma(fma(q22, e2, B), e2, A) (A, B once per row), and the exp / FMA
+//   part runs only when some lane of the warp is inside the 3-sigma cutoff.
+//   Forward: per-warp partial tiles are summed through shared memory once
+//   per tile and stored as complex64.  Backward: per (tile, Gaussian) a
+//   lane folds its voxels into 11 moments, the warp reduce-scatters them
+//   (16 shuffles) and lanes issue one atomic per moment (or, deterministic,
+//   write the per-pair partial for a fixed-order reduction in finalize).
+//
+// Other tile edges use a generic one-voxel-per-thread kernel pair.
+//
+// Reference semantics (3DGS/3dgsVC/gaussian/cuda_ext/tile_voxelize_cuda_kernel.cu):
+//   forward  :118-141  vol = sum_{g in list(tile), m <= 9} exp(-m/2) rho_g
+//   backward :217-252  dL/drho, dL/dcenter, dL/dcov_inv for included pairs
+#include <cstdio>
+
+#include "gsv_common.cuh"
+
+using namespace gsv;
+
+namespace gsv {
+int layout_for(gsv_shape shape, int64_t n, int64_t cap, int flags, GaussLayout* G, PairLayout* P,
+               int64_t* ntiles);
+}
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 4;
+constexpr int kThreads = kWarps * 32;
+
+struct RenderArgs {
+    // native Gaussians
+    const Rec* recs;
+    // reference-compatible Gaussians
+    const float* centers;
+    const float* cov_inv;
+    const float* den_r;
+    const float* den_i;
+    const float* half_shape;
+    // binning
+    const int2* ranges;
+    const int32_t* pair_ids;
+    int32_t d, h, w, ts, nth, ntw;
+    int64_t ntiles;
+    float hs[3], ih[3];  // native half shape and its reciprocal
+    // forward outputs
+    float* vol;    // complex64 interleaved
+    float* vol_r;  // planar
+    float* vol_i;
+    // backward inputs / outputs
+    const float* gvol;  // complex64 interleaved
+    const float* gv_r;  // planar
+    const float* gv_i;
+    float* accum;     // [n, 12] moments (native, atomics)
+    float* partials;  // [pairs, 12] moments (native, deterministic)
+    float* g_center;  // compat outputs
+    float* g_cov;
+    float* g_dr;
+    float* g_di;
+};
+
+template <bool COMPAT>
+__device__ __forceinline__ void compat_ih(const RenderArgs& a, float ih[3]) {
+    if (COMPAT) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ih[k] = __fdiv_rn(1.0f, __ldg(a.half_shape + k));
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ih[k] = a.ih[k];
+    }
+}
+
+template <bool COMPAT>
+__device__ __forceinline__ Rec load_rec(const RenderArgs& a, int gid, const float ih[3]) {
+    Rec r;
+    if (!COMPAT) {
+        const float4* p = reinterpret_cast<const float4*>(a.recs + gid);
+        const float4 x = __ldg(p), y = __ldg(p + 1), z = __ldg(p + 2);
+        r.c0 = x.x; r.c1 = x.y; r.c2 = x.z; r.q00 = x.w;
+        r.q01x2 = y.x; r.q02x2 = y.y; r.q11 = y.z; r.q12x2 = y.w;
+        r.q22 = z.x; r.rho_r = z.y; r.rho_i = z.z; r.pad = 0.0f;
+    } else {
+        float m9[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) m9[k] = __ldg(a.cov_inv + int64_t(gid) * 9 + k);
+        float qc[6];
+        qcoef_from_covinv(m9, ih, qc);
+        r.c0 = __ldg(a.centers + int64_t(gid) * 3);
+        r.c1 = __ldg(a.centers + int64_t(gid) * 3 + 1);
+        r.c2 = __ldg(a.centers + int64_t(gid) * 3 + 2);
+        r.q00 = qc[0]; r.q01x2 = qc[1]; r.q02x2 = qc[2]; r.q11 = qc[3]; r.q12x2 = qc[4]; r.q22 = qc[5];
+        r.rho_r = __ldg(a.den_r + gid);
+        r.rho_i = __ldg(a.den_i + gid);
+        r.pad = 0.0f;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void decode_tile(const RenderArgs& a, int64_t tile, int& d0, int& h0, int& w0) {
+    const int64_t per = int64_t(a.nth) * a.ntw;
+    d0 = int(tile / per) * a.ts;
+    const int64_t rem = tile % per;
+    h0 = int(rem / a.ntw) * a.ts;
+    w0 = int(rem % a.ntw) * a.ts;
+}
+
+// Reduce-scatter of 16 per-lane values over the warp: afterwards lane l
+// holds the warp total of value (l >> 1) in v[0] (lanes l and l^1 agree).
+__device__ __forceinline__ float warp_reduce_scatter16(float v[16], int lane) {
+    {
+        const bool hi = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float send = hi ? v[i] : v[i + 8];
+            const float keep = hi ? v[i + 8] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 16);
+        }
+    }
+    {
+        const bool hi = lane & 8;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float send = hi ? v[i] : v[i + 4];
+            const float keep = hi ? v[i + 4] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 8);
+        }
+    }
+    {
+        const bool hi = lane & 4;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const float send = hi ? v[i] : v[i + 2];
+            const float keep = hi ? v[i + 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 4);
+        }
+    }
+    {
+        const bool hi = lane & 2;
+        const float send = hi ? v[0] : v[1];
+        const float keep = hi ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(kFull, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(kFull, v[0], 1);
+}
+
+// Compat outputs for one (tile, Gaussian): every lane holds `tot` (lane 2i
+// holds moment i); lanes 0..13 issue one atomic each.
+__device__ __forceinline__ void compat_emit(const RenderArgs& a, const Rec& g, int gid, float tot,
+                                            int lane, const float ih[3]) {
+    float m[kMom];
+#pragma unroll
+    for (int i = 0; i < kMom; ++i) m[i] = __shfl_sync(kFull, tot, 2 * i);
+    float out;
+    switch (lane) {
+        case 0: out = m[0]; break;
+        case 1: out = m[1]; break;
+        // dL/dcenter_a = -2 sum_b Q_ab S1_b   (reference: -2 (M d)_a / hs_a, .cu:241-243)
+        case 2: out = -(2.0f * g.q00 * m[2] + g.q01x2 * m[3] + g.q02x2 * m[4]); break;
+        case 3: out = -(g.q01x2 * m[2] + 2.0f * g.q11 * m[3] + g.q12x2 * m[4]); break;
+        case 4: out = -(g.q02x2 * m[2] + g.q12x2 * m[3] + 2.0f * g.q22 * m[4]); break;
+        // dL/dcov_inv_ab = sum a d_a d_b = S2_ab / (hs_a hs_b)  (.cu:244-252)
+        case 5: out = m[5] * ih[0] * ih[0]; break;
+        case 6: case 8: out = m[6] * ih[0] * ih[1]; break;
+        case 7: case 11: out = m[7] * ih[0] * ih[2]; break;
+        case 9: out = m[8] * ih[1] * ih[1]; break;
+        case 10: case 12: out = m[9] * ih[1] * ih[2]; break;
+        case 13: out = m[10] * ih[2] * ih[2]; break;
+        default: out = 0.0f; break;
+    }
+    if (lane == 0) atomicAdd(a.g_dr + gid, out);
+    else if (lane == 1) atomicAdd(a.g_di + gid, out);
+    else if (lane < 5) atomicAdd(a.g_center + int64_t(gid) * 3 + (lane - 2), out);
+    else if (lane < 14) {
+        // lanes 5..13 -> cov entries 0..8 in row-major order
+        const int e = lane - 5;
+        atomicAdd(a.g_cov + int64_t(gid) * 9 + e, out);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile edge 8: forward
+// ---------------------------------------------------------------------------
+
+struct __align__(16) WarpStage {
+    Rec rec[32];
+    float4 e2[32][2];
+    int32_t gid[32];
+};
+
+template <bool COMPAT, bool PLANAR>
+__global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
+    __shared__ __align__(16) unsigned char smem_raw[kWarps * 16 * 32 * sizeof(float2)];
+    WarpStage* stage = reinterpret_cast<WarpStage*>(smem_raw);
+    static_assert(sizeof(WarpStage) * kWarps <= sizeof(smem_raw), "stage too large");
+
+    const int64_t tile = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    const int2 rg = a.ranges[tile];
+
+    float accR[16], accI[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) accR[k] = accI[k] = 0.0f;
+
+    if (rg.x < rg.y) {
+        float ih[3];
+        compat_ih<COMPAT>(a, ih);
+        const float ev0a = float(d0 + (lane >> 3));
+        const float ev0b = float(d0 + 4 + (lane >> 3));
+        const float ev1 = float(h0 + (lane & 7));
+        WarpStage& S = stage[warp];
+        for (int base = rg.x + warp * 32; base < rg.y; base += kWarps * 32) {
+            const int cnt = min(32, rg.y - base);
+            if (lane < cnt) {
+                const int gid = __ldg(a.pair_ids + base + lane);
+                const Rec r = load_rec<COMPAT>(a, gid, ih);
+                S.rec[lane] = r;
+                float e2[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
+                S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
+                S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
+            }
+            __syncwarp();
+            for (int j = 0; j < cnt; ++j) {
+                const Rec g = S.rec[j];
+                const float4 ea = S.e2[j][0], eb = S.e2[j][1];
+                const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
+                const float e1 = __fsub_rn(ev1, g.c1);
+                const float e0a = __fsub_rn(ev0a, g.c0);
+                const float e0b = __fsub_rn(ev0b, g.c0);
+                const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
+                const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
+                float m[16];
+                bool any = false;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    m[k] = row_m(g.q22, Aa, Ba, e2[k]);
+                    m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
+                    any |= (m[k] <= kCut) | (m[8 + k] <= kCut);
+                }
+                if (__any_sync(kFull, any)) {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        if (m[k] <= kCut) {
+                            const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
+                            accR[k] = fmaf(wgt, g.rho_r, accR[k]);
+                            accI[k] = fmaf(wgt, g.rho_i, accI[k]);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+
+    // Sum the four warps' partial tiles: red[(warp*16 + k)*32 + lane].
+    __syncthreads();
+    float2* red = reinterpret_cast<float2*>(smem_raw);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) red[(warp * 16 + k) * 32 + lane] = make_float2(accR[k], accI[k]);
+    __syncthreads();
+
+    // Thread t stores voxels 4t..4t+3 of the tile (row t/2, columns (t%2)*4..+3).
+    const int t = threadIdx.x;
+    const int row = t >> 1;           // 0..63 = ld*8 + lh
+    const int ld = row >> 3, lh = row & 7, lw0 = (t & 1) * 4;
+    const int src_lane = row & 31, slot = row >> 5;
+    float2 v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int k = slot * 8 + lw0 + i;
+        float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int wv = 0; wv < kWarps; ++wv) {
+            const float2 x = red[(wv * 16 + k) * 32 + src_lane];
+            s.x += x.x;
+            s.y += x.y;
+        }
+        v[i] = s;
+    }
+    const int gd = d0 + ld, gh = h0 + lh, gw = w0 + lw0;
+    if (gd >= a.d || gh >= a.h) return;
+    const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
+    if (PLANAR) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (gw + i < a.w) {
+                a.vol_r[flat + i] = v[i].x;
+                a.vol_i[flat + i] = v[i].y;
+            }
+    } else {
+        float2* out = reinterpret_cast<float2*>(a.vol) + flat;
+        if (gw + 3 < a.w && (a.w & 1) == 0) {
+            float4* o4 = reinterpret_cast<float4*>(out);
+            o4[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+            o4[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (gw + i < a.w) out[i] = v[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile edge 8: backward
+// ---------------------------------------------------------------------------
+
+template <bool COMPAT, bool DET>
+__global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
+    __shared__ __align__(16) WarpStage stage[kWarps];
+
+    const int64_t tile = blockIdx.x;
+    const int2 rg = a.ranges[tile];
+    if (rg.x >= rg.y) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    float ih[3];
+    compat_ih<COMPAT>(a, ih);
+
+    // Upstream gradient of the lane's 16 voxels (zero outside the volume).
+    float gr[16], gi[16];
+    {
+        const int gh = h0 + (lane & 7);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int gd = d0 + r * 4 + (lane >> 3);
+            const bool row_ok = gd < a.d && gh < a.h;
+            const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + w0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const bool ok = row_ok && (w0 + k < a.w);
+                if (COMPAT) {
+                    gr[r * 8 + k] = ok ? __ldg(a.gv_r + flat + k) : 0.0f;
+                    gi[r * 8 + k] = ok ? __ldg(a.gv_i + flat + k) : 0.0f;
+                } else {
+                    const float2 x = ok ? __ldg(reinterpret_cast<const float2*>(a.gvol) + flat + k)
+                                        : make_float2(0.f, 0.f);
+                    gr[r * 8 + k] = x.x;
+                    gi[r * 8 + k] = x.y;
+                }
+            }
+        }
+    }
+
+    const float ev0a = float(d0 + (lane >> 3));
+    const float ev0b = float(d0 + 4 + (lane >> 3));
+    const float ev1 = float(h0 + (lane & 7));
+    WarpStage& S = stage[warp];
+    for (int base = rg.x + warp * 32; base < rg.y; base += kWarps * 32) {
+        const int cnt = min(32, rg.y - base);
+        if (lane < cnt) {
+            const int gid = __ldg(a.pair_ids + base + lane);
+            const Rec r = load_rec<COMPAT>(a, gid, ih);
+            S.rec[lane] = r;
+            S.gid[lane] = gid;
+            float e2[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
+            S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
+            S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
+        }
+        __syncwarp();
+        for (int j = 0; j < cnt; ++j) {
+            const Rec g = S.rec[j];
+            const float4 ea = S.e2[j][0], eb = S.e2[j][1];
+            const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
+            const float e1 = __fsub_rn(ev1, g.c1);
+            const float e0a = __fsub_rn(ev0a, g.c0);
+            const float e0b = __fsub_rn(ev0b, g.c0);
+            const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
+            const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
+            float m[16];
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                m[k] = row_m(g.q22, Aa, Ba, e2[k]);
+                m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
+                any |= (m[k] <= kCut) | (m[8 + k] <= kCut);
+            }
+            if (!__any_sync(kFull, any)) continue;
+            const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
+            float R0[2] = {0.f, 0.f}, R1[2] = {0.f, 0.f}, R2[2] = {0.f, 0.f};
+            float Dr = 0.f, Di = 0.f;
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int q = r * 8 + k;
+                    if (m[q] <= kCut) {
+                        const float wgt = ex2_approx(m[q] * kNegHalfLog2e);
+                        const float av = wgt * fmaf(hi, gi[q], hr * gr[q]);
+                        Dr = fmaf(wgt, gr[q], Dr);
+                        Di = fmaf(wgt, gi[q], Di);
+                        R0[r] += av;
+                        const float ae = av * e2[k];
+                        R1[r] += ae;
+                        R2[r] = fmaf(ae, e2[k], R2[r]);
+                    }
+                }
+            }
+            float v[16];
+            const float R0s = R0[0] + R0[1];
+            v[0] = Dr;
+            v[1] = Di;
+            v[2] = fmaf(e0a, R0[0], e0b * R0[1]);
+            v[3] = e1 * R0s;
+            v[4] = R1[0] + R1[1];
+            v[5] = fmaf(e0a * e0a, R0[0], (e0b * e0b) * R0[1]);
+            v[6] = e1 * v[2];
+            v[7] = fmaf(e0a, R1[0], e0b * R1[1]);
+            v[8] = (e1 * e1) * R0s;
+            v[9] = e1 * v[4];
+            v[10] = R2[0] + R2[1];
+#pragma unroll
+            for (int i = 11; i < 16; ++i) v[i] = 0.f;
+            const float tot = warp_reduce_scatter16(v, lane);
+            const int gid = S.gid[j];
+            if (COMPAT) {
+                compat_emit(a, g, gid, tot, lane, ih);
+            } else if (DET) {
+                if (!(lane & 1) && (lane >> 1) < kMom)
+                    a.partials[int64_t(base + j) * kMomStride + (lane >> 1)] = tot;
+            } else {
+                if (!(lane & 1) && (lane >> 1) < kMom)
+                    atomicAdd(a.accum + int64_t(gid) * kMomStride + (lane >> 1), tot);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Generic tile edge: one voxel per thread, Gaussians staged per CTA.
+// ---------------------------------------------------------------------------
+
+template <bool COMPAT, bool PLANAR>
+__global__ void __launch_bounds__(kThreads) k_forward_generic(const RenderArgs a) {
+    __shared__ Rec srec[kThreads];
+    const int64_t tile = blockIdx.x;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    const int2 rg = a.ranges[tile];
+    const int ts = a.ts;
+    const int nvox = ts * ts * ts;
+    float ih[3];
+    compat_ih<COMPAT>(a, ih);
+    for (int c0 = 0; c0 < nvox; c0 += kThreads) {  // uniform trip count
+        const int vid = c0 + threadIdx.x;
+        const int ld = vid / (ts * ts), lh = (vid / ts) % ts, lw = vid % ts;
+        const int gd = d0 + ld, gh = h0 + lh, gw = w0 + lw;
+        const bool valid = vid < nvox && gd < a.d && gh < a.h && gw < a.w;
+        const float v0 = float(gd), v1 = float(gh), v2 = float(gw);
+        float ar = 0.f, ai = 0.f;
+        for (int base = rg.x; base < rg.y; base += kThreads) {  // uniform trip count
+            const int cnt = min(kThreads, rg.y - base);
+            __syncthreads();
+            if (threadIdx.x < cnt) srec[threadIdx.x] = load_rec<COMPAT>(a, __ldg(a.pair_ids + base + threadIdx.x), ih);
+            __syncthreads();
+            for (int j = 0; j < cnt; ++j) {
+                const Rec g = srec[j];
+                const float e0 = __fsub_rn(v0, g.c0), e1 = __fsub_rn(v1, g.c1), e2 = __fsub_rn(v2, g.c2);
+                const float m = row_m(g.q22, row_a(g, e0, e1), row_b(g, e0, e1), e2);
+                if (m <= kCut) {
+                    const float wgt = ex2_approx(m * kNegHalfLog2e);
+                    ar = fmaf(wgt, g.rho_r, ar);
+                    ai = fmaf(wgt, g.rho_i, ai);
+                }
+            }
+        }
+        if (valid) {
+            const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
+            if (PLANAR) {
+                a.vol_r[flat] = ar;
+                a.vol_i[flat] = ai;
+            } else {
+                reinterpret_cast<float2*>(a.vol)[flat] = make_float2(ar, ai);
+            }
+        }
+    }
+}
+
+template <bool COMPAT, bool DET>
+__global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs a) {
+    __shared__ Rec srec[32];
+    __shared__ int sgid[32];
+    __shared__ float sred[kWarps][kMom];
+    const int64_t tile = blockIdx.x;
+    const int2 rg = a.ranges[tile];
+    if (rg.x >= rg.y) return;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    const int ts = a.ts;
+    const int nvox = ts * ts * ts;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float ih[3];
+    compat_ih<COMPAT>(a, ih);
+    for (int base = rg.x; base < rg.y; base += 32) {
+        const int cnt = min(32, rg.y - base);
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            const int gid = __ldg(a.pair_ids + base + threadIdx.x);
+            sgid[threadIdx.x] = gid;
+            srec[threadIdx.x] = load_rec<COMPAT>(a, gid, ih);
+        }
+        __syncthreads();
+        for (int j = 0; j < cnt; ++j) {
+            const Rec g = srec[j];
+            float v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = 0.f;
+            for (int vid = threadIdx.x; vid < nvox; vid += kThreads) {
+                const int ld = vid / (ts * ts), lh = (vid / ts) % ts, lw = vid % ts;
+                const int gd = d0 + ld, gh = h0 + lh, gw = w0 + lw;
+                if (gd >= a.d || gh >= a.h || gw >= a.w) continue;
+                const float e0 = __fsub_rn(float(gd), g.c0), e1 = __fsub_rn(float(gh), g.c1);
+                const float e2 = __fsub_rn(float(gw), g.c2);
+                const float m = row_m(g.q22, row_a(g, e0, e1), row_b(g, e0, e1), e2);
+                if (!(m <= kCut)) continue;
+                const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
+                float gr, gi;
+                if (COMPAT) {
+                    gr = __ldg(a.gv_r + flat);
+                    gi = __ldg(a.gv_i + flat);
+                } else {
+                    const float2 x = __ldg(reinterpret_cast<const float2*>(a.gvol) + flat);
+                    gr = x.x;
+                    gi = x.y;
+                }
+                const float wgt = ex2_approx(m * kNegHalfLog2e);
+                const float av = wgt * fmaf(-0.5f * g.rho_i, gi, (-0.5f * g.rho_r) * gr);
+                v[0] = fmaf(wgt, gr, v[0]);
+                v[1] = fmaf(wgt, gi, v[1]);
+                v[2] = fmaf(av, e0, v[2]);
+                v[3] = fmaf(av, e1, v[3]);
+                v[4] = fmaf(av, e2, v[4]);
+                v[5] = fmaf(av * e0, e0, v[5]);
+                v[6] = fmaf(av * e0, e1, v[6]);
+                v[7] = fmaf(av * e0, e2, v[7]);
+                v[8] = fmaf(av * e1, e1, v[8]);
+                v[9] = fmaf(av * e1, e2, v[9]);
+                v[10] = fmaf(av * e2, e2, v[10]);
+            }
+            const float tot = warp_reduce_scatter16(v, lane);
+            if (!(lane & 1) && (lane >> 1) < kMom) sred[warp][lane >> 1] = tot;
+            __syncthreads();
+            // warp 0 combines the four warps in a fixed order
+            if (warp == 0) {
+                float t = 0.f;
+                if (lane < kMom) t = ((sred[0][lane] + sred[1][lane]) + sred[2][lane]) + sred[3][lane];
+                // compat_emit expects moment i in lane 2i
+                const float spread = __shfl_sync(kFull, t, lane >> 1);
+                const int gid = sgid[j];
+                if (COMPAT) {
+                    compat_emit(a, g, gid, spread, lane, ih);
+                } else if (DET) {
+                    if (lane < kMom) a.partials[int64_t(base + j) * kMomStride + lane] = t;
+                } else {
+                    if (lane < kMom) atomicAdd(a.accum + int64_t(gid) * kMomStride + lane, t);
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Finalize: moments -> dL/d(positions, scales, rotations, density).
+// Chain rule of tile_voxelizer.py:284-290 and :77-84 (the torch autograd
+// tail of the reference), in FP32.
+// ---------------------------------------------------------------------------
+
+template <bool DET>
+__global__ void __launch_bounds__(256) k_finalize(const gsv_params p, const RenderArgs a,
+                                                  const int4* __restrict__ boxes,
+                                                  gsv_grads out) {
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= p.n) return;
+    float mo[kMom];
+    if (!DET) {
+#pragma unroll
+        for (int i = 0; i < kMom; ++i) mo[i] = a.accum[g * kMomStride + i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < kMom; ++i) mo[i] = 0.f;
+        const int4 b = boxes[g];
+        const int t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
+        const int n0 = (b.y >> 16) & 0xffff, n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
+        if (b.w > 0) {
+            for (int i = 0; i < n0; ++i)
+                for (int j = 0; j < n1; ++j)
+                    for (int k = 0; k < n2; ++k) {
+                        const int64_t t = (int64_t(t0 + i) * a.nth + (t1 + j)) * a.ntw + (t2 + k);
+                        const int2 rg = a.ranges[t];
+                        int lo = rg.x, hi = rg.y;  // pair_ids ascending within the tile
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (a.pair_ids[mid] < int(g)) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        if (lo < rg.y && a.pair_ids[lo] == int(g)) {
+                            const float* src = a.partials + int64_t(lo) * kMomStride;
+#pragma unroll
+                            for (int q = 0; q < kMom; ++q) mo[q] += src[q];
+                        }
+                    }
+        }
+    }
+    const Rec R = a.recs[g];
+    // dL/dcenter_vox, then dcenter/dpositions = 0.5 * shape = hs   (:284)
+    const float dc0 = -(2.0f * R.q00 * mo[2] + R.q01x2 * mo[3] + R.q02x2 * mo[4]);
+    const float dc1 = -(R.q01x2 * mo[2] + 2.0f * R.q11 * mo[3] + R.q12x2 * mo[4]);
+    const float dc2 = -(R.q02x2 * mo[2] + R.q12x2 * mo[3] + 2.0f * R.q22 * mo[4]);
+    out.positions[g * 3 + 0] = dc0 * a.hs[0];
+    out.positions[g * 3 + 1] = dc1 * a.hs[1];
+    out.positions[g * 3 + 2] = dc2 * a.hs[2];
+    out.density_r[g] = mo[0];
+    out.density_i[g] = mo[1];
+    // dL/dM (normalised units), symmetric.
+    float G[9];
+    G[0] = mo[5] * a.ih[0] * a.ih[0];
+    G[1] = G[3] = mo[6] * a.ih[0] * a.ih[1];
+    G[2] = G[6] = mo[7] * a.ih[0] * a.ih[2];
+    G[4] = mo[8] * a.ih[1] * a.ih[1];
+    G[5] = G[7] = mo[9] * a.ih[1] * a.ih[2];
+    G[8] = mo[10] * a.ih[2] * a.ih[2];
+    // Rebuild R(qn), si = 1/(s+1e-8) and T = R diag(si).
+    float q[4], s[3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) q[k] = p.rotations[g * 4 + k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s[k] = p.scales[g * 3 + k];
+    const float nrm = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    const float den = nrm + 1e-8f;
+    const float w = q[0] / den, x = q[1] / den, y = q[2] / den, z = q[3] / den;
+    float r[9];
+    r[0] = 1.f - 2.f * y * y - 2.f * z * z;
+    r[1] = 2.f * x * y - 2.f * z * w;
+    r[2] = 2.f * x * z + 2.f * y * w;
+    r[3] = 2.f * x * y + 2.f * z * w;
+    r[4] = 1.f - 2.f * x * x - 2.f * z * z;
+    r[5] = 2.f * y * z - 2.f * x * w;
+    r[6] = 2.f * x * z - 2.f * y * w;
+    r[7] = 2.f * y * z + 2.f * x * w;
+    r[8] = 1.f - 2.f * x * x - 2.f * y * y;
+    float si[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) si[j] = 1.0f / (s[j] + 1e-8f);
+    // dL/dT = (G + G^T) T = 2 G T
+    float gr[9], gsi[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += G[i * 3 + k] * (r[k * 3 + j] * si[j]);
+            const float gt = 2.0f * acc;
+            gr[i * 3 + j] = gt * si[j];
+            gsi[j] += gt * r[i * 3 + j];
+        }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) out.scales[g * 3 + j] = -gsi[j] * si[j] * si[j];
+    float gn[4];
+    gn[0] = 2.f * (-z * gr[1] + y * gr[2] + z * gr[3] - x * gr[5] - y * gr[6] + x * gr[7]);
+    gn[1] = 2.f * (y * gr[1] + z * gr[2] + y * gr[3] - 2.f * x * gr[4] - w * gr[5] + z * gr[6] + w * gr[7] -
+                   2.f * x * gr[8]);
+    gn[2] = 2.f * (-2.f * y * gr[0] + x * gr[1] + w * gr[2] + x * gr[3] + z * gr[5] - w * gr[6] + z * gr[7] -
+                   2.f * y * gr[8]);
+    gn[3] = 2.f * (-2.f * z * gr[0] - w * gr[1] + x * gr[2] + w * gr[3] - 2.f * z * gr[4] + y * gr[5] +
+                   x * gr[6] + y * gr[7]);
+    const float dot = gn[0] * w + gn[1] * x + gn[2] * y + gn[3] * z;
+    const float corr = nrm > 0.f ? dot / (nrm * den) : 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out.rotations[g * 4 + k] = gn[k] / den - q[k] * corr;
+}
+
+int grid_for(int64_t items, int block) {
+    int64_t g = (items + block - 1) / block;
+    return int(g < 1 ? 1 : g);
+}
+
+template <typename T>
+const T* cat(const void* base, size_t off) {
+    return reinterpret_cast<const T*>(static_cast<const char*>(base) + off);
+}
+template <typename T>
+T* mat(void* base, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(base) + off);
+}
+
+void fill_shape(RenderArgs& a, gsv_shape s) {
+    a.d = s.d; a.h = s.h; a.w = s.w; a.ts = s.tile_size;
+    a.nth = (s.h + s.tile_size - 1) / s.tile_size;
+    a.ntw = (s.w + s.tile_size - 1) / s.tile_size;
+    a.ntiles = int64_t((s.d + s.tile_size - 1) / s.tile_size) * a.nth * a.ntw;
+    const float sh[3] = {float(s.d), float(s.h), float(s.w)};
+    for (int k = 0; k < 3; ++k) {
+        a.hs[k] = sh[k] * 0.5f;
+        a.ih[k] = 1.0f / a.hs[k];
+    }
+}
+
+bool shape_ok(int32_t ts, int32_t d, int32_t h, int32_t w) {
+    return ts > 0 && d > 0 && h > 0 && w > 0 && d < (1 << 24) && h < (1 << 24) && w < (1 << 24);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,
+                int64_t capacity, float* volume, void* stream) {
+    GaussLayout G;
+    PairLayout P;
+    int64_t ntiles = 0;
+    if (layout_for(shape, n, capacity, 0, &G, &P, &ntiles) != GSV_OK || !ws_gauss || !volume ||
+        (capacity > 0 && !ws_pairs))
+        return GSV_ERR_INVALID_ARGUMENT;
+    if (ntiles > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RenderArgs a{};
+    fill_shape(a, shape);
+    a.recs = cat<Rec>(ws_gauss, G.rec);
+    a.ranges = cat<int2>(ws_gauss, G.ranges);
+    a.pair_ids = capacity > 0 ? cat<int32_t>(ws_pairs, P.vals_out) : nullptr;
+    a.vol = volume;
+    if (shape.tile_size == 8) k_forward8<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+    else k_forward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+int gsv_backward(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* ws_pairs,
+                 int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
+                 void* stream) {
+    GaussLayout G;
+    PairLayout P;
+    int64_t ntiles = 0;
+    const bool det = flags & GSV_BACKWARD_DETERMINISTIC;
+    if (!p || !grads || layout_for(shape, p->n, capacity, flags, &G, &P, &ntiles) != GSV_OK || !ws_gauss ||
+        !grad_volume || (capacity > 0 && !ws_pairs))
+        return GSV_ERR_INVALID_ARGUMENT;
+    const int64_t n = p->n;
+    if (n == 0) return GSV_OK;
+    if (!grads->positions || !grads->scales || !grads->rotations || !grads->density_r || !grads->density_i ||
+        !p->scales || !p->rotations)
+        return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RenderArgs a{};
+    fill_shape(a, shape);
+    a.recs = cat<Rec>(ws_gauss, G.rec);
+    a.ranges = cat<int2>(ws_gauss, G.ranges);
+    a.pair_ids = capacity > 0 ? cat<int32_t>(ws_pairs, P.vals_out) : nullptr;
+    a.gvol = grad_volume;
+    a.accum = mat<float>(ws_gauss, G.accum);
+    a.partials = det ? mat<float>(ws_pairs, P.partials) : nullptr;
+    if (det) {
+        if (capacity > 0)
+            GSV_CUDA_TRY(cudaMemsetAsync(a.partials, 0, size_t(capacity) * kMomStride * sizeof(float), st));
+    } else {
+        GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
+    }
+    if (capacity > 0) {
+        if (shape.tile_size == 8) {
+            if (det) k_backward8<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            else k_backward8<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+        } else {
+            if (det) k_backward_generic<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            else k_backward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+        }
+        GSV_LAUNCH_CHECK();
+    }
+    if (det) k_finalize<true><<<grid_for(n, 256), 256, 0, st>>>(*p, a, cat<int4>(ws_gauss, G.box), *grads);
+    else k_finalize<false><<<grid_for(n, 256), 256, 0, st>>>(*p, a, cat<int4>(ws_gauss, G.box), *grads);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+int gsv_tile_forward(const float* centers, const float* cov_inv, const float* density_r,
+                     const float* density_i, const int32_t* tile_ranges, const int32_t* pair_ids,
+                     const float* half_shape, int64_t n, int64_t num_tiles, int32_t tile_size,
+                     int32_t d, int32_t h, int32_t w, float* vol_r, float* vol_i, void* stream) {
+    if (!shape_ok(tile_size, d, h, w) || n < 0 || !tile_ranges || !half_shape || !vol_r || !vol_i)
+        return GSV_ERR_INVALID_ARGUMENT;
+    gsv_shape s{d, h, w, tile_size};
+    RenderArgs a{};
+    fill_shape(a, s);
+    if (num_tiles != a.ntiles || num_tiles > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    if (n > 0 && (!centers || !cov_inv || !density_r || !density_i)) return GSV_ERR_INVALID_ARGUMENT;
+    a.centers = centers;
+    a.cov_inv = cov_inv;
+    a.den_r = density_r;
+    a.den_i = density_i;
+    a.half_shape = half_shape;
+    a.ranges = reinterpret_cast<const int2*>(tile_ranges);
+    a.pair_ids = pair_ids;
+    a.vol_r = vol_r;
+    a.vol_i = vol_i;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (tile_size == 8) k_forward8<true, true><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    else k_forward_generic<true, true><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+int gsv_tile_backward(const float* centers, const float* cov_inv, const float* density_r,
+                      const float* density_i, const int32_t* tile_ranges, const int32_t* pair_ids,
+                      const float* half_shape, const float* grad_vol_r, const float* grad_vol_i,
+                      int64_t n, int64_t num_tiles, int32_t tile_size, int32_t d, int32_t h,
+                      int32_t w, float* grad_centers, float* grad_cov_inv, float* grad_den_r,
+                      float* grad_den_i, void* stream) {
+    if (!shape_ok(tile_size, d, h, w) || n < 0 || !tile_ranges || !half_shape || !grad_vol_r ||
+        !grad_vol_i)
+        return GSV_ERR_INVALID_ARGUMENT;
+    gsv_shape s{d, h, w, tile_size};
+    RenderArgs a{};
+    fill_shape(a, s);
+    if (num_tiles != a.ntiles || num_tiles > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    if (n == 0) return GSV_OK;
+    if (!centers || !cov_inv || !density_r || !density_i || !grad_centers || !grad_cov_inv ||
+        !grad_den_r || !grad_den_i)
+        return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GSV_CUDA_TRY(cudaMemsetAsync(grad_centers, 0, size_t(n) * 3 * sizeof(float), st));
+    GSV_CUDA_TRY(cudaMemsetAsync(grad_cov_inv, 0, size_t(n) * 9 * sizeof(float), st));
+    GSV_CUDA_TRY(cudaMemsetAsync(grad_den_r, 0, size_t(n) * sizeof(float), st));
+    GSV_CUDA_TRY(cudaMemsetAsync(grad_den_i, 0, size_t(n) * sizeof(float), st));
+    a.centers = centers;
+    a.cov_inv = cov_inv;
+    a.den_r = density_r;
+    a.den_i = density_i;
+    a.half_shape = half_shape;
+    a.ranges = reinterpret_cast<const int2*>(tile_ranges);
+    a.pair_ids = pair_ids;
+    a.gv_r = grad_vol_r;
+    a.gv_i = grad_vol_i;
+    a.g_center = grad_centers;
+    a.g_cov = grad_cov_inv;
+    a.g_dr = grad_den_r;
+    a.g_di = grad_den_i;
+    if (tile_size == 8) k_backward8<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    else k_backward_generic<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,187 @@
+/*
+ * gsv.h -- C ABI of the B200 (sm_100a) complex-Gaussian tile voxelizer.
+ *
+ * Plain pointers, sizes and a CUDA stream handle; no torch types.  Every
+ * device pointer is caller-owned.  Every entry point only enqueues work on
+ * `stream` (no host synchronisation) unless its comment says otherwise, so a
+ * sequence of calls can be captured in a CUDA graph.
+ *
+ * Reference interfaces replaced (paths relative to the 3DGSMR project root,
+ * V = 3DGS/3dgsVC):
+ *   gsv_tile_forward            V/gaussian/cuda_ext/tile_voxelize_cuda.cpp:5-16,33-34
+ *                               (tile_voxelize_forward_cuda, tile_voxelize_cuda_kernel.cu:262-300)
+ *   gsv_tile_backward           V/gaussian/cuda_ext/tile_voxelize_cuda.cpp:18-31,35
+ *                               (tile_voxelize_backward_cuda, tile_voxelize_cuda_kernel.cu:302-349)
+ *   gsv_build_tile_pairs_count  V/gaussian/tile_voxelizer.py:87-118  (build_tile_pairs, up to the
+ *                               host read of the pair total)
+ *   gsv_build_tile_pairs_fill   V/gaussian/tile_voxelizer.py:120-162 (build_tile_pairs, rest)
+ *   gsv_prepare / gsv_bin       V/gaussian/tile_voxelizer.py:282-293 (TileVoxelizer.forward
+ *                               preprocess + binning, fused)
+ *   gsv_forward                 V/gaussian/tile_voxelizer.py:296-309 (_TileVoxelizeCUDA.forward)
+ *   gsv_backward                V/gaussian/tile_voxelizer.py:188-207 (_TileVoxelizeCUDA.backward)
+ *                               fused with the torch autograd chain of :284-290 and :77-84
+ *
+ * Conventions
+ *   - Volumes are (D,H,W) row-major.  Native volumes are complex64
+ *     (interleaved re,im float pairs); the reference-compatible entry points
+ *     use two float planes as the reference extension does.
+ *   - positions [n,3] in [-1,1] (axis order d,h,w), scales [n,3] (the
+ *     exp of the log-scale parameter, a fraction of the half extent),
+ *     rotations [n,4] (w,x,y,z, unnormalised), density re/im [n]:
+ *     the parameter layout of V/gaussian/gaussian_model.py:38-68.
+ *   - Return value: a gsv_status.  Launch and argument errors are reported
+ *     immediately; data-dependent conditions found on the device
+ *     (capacity overflow, empty boxes) are latched in the workspace status
+ *     word and read back with gsv_read_status.
+ */
+#ifndef GSV_H_
+#define GSV_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GSV_API __attribute__((visibility("default")))
+#else
+#define GSV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSV_ABI_VERSION 1
+
+typedef enum gsv_status {
+    GSV_OK = 0,
+    GSV_ERR_INVALID_ARGUMENT = 1, /* bad shape, size, null pointer or workspace too small */
+    GSV_ERR_CAPACITY = 2,         /* more (tile, Gaussian) pairs than the pair capacity */
+    GSV_ERR_CUDA = 3,             /* a CUDA runtime call or launch failed */
+    GSV_ERR_EMPTY_BOX = 4,        /* a Gaussian's tile box is empty (negative radius) */
+    GSV_ERR_TOO_MANY_PAIRS = 5    /* pair total exceeds INT32_MAX (int32 tile ranges) */
+} gsv_status;
+
+/* Device-latched status bits (gsv_read_status). */
+#define GSV_FLAG_CAPACITY_OVERFLOW 0x1
+#define GSV_FLAG_EMPTY_BOX 0x2
+#define GSV_FLAG_TOO_MANY_PAIRS 0x4
+
+/* Backward options. */
+#define GSV_BACKWARD_DETERMINISTIC 0x1 /* fixed-order reduction: bitwise reproducible gradients */
+
+typedef struct gsv_shape {
+    int32_t d, h, w;   /* volume extent in voxels */
+    int32_t tile_size; /* cubic binning tile edge (the reference's `tile_size`) */
+} gsv_shape;
+
+typedef struct gsv_params { /* device pointers, FP32, contiguous */
+    const float* positions;
+    const float* scales;
+    const float* rotations;
+    const float* density_r;
+    const float* density_i;
+    int64_t n;
+} gsv_params;
+
+typedef struct gsv_grads { /* device pointers, FP32, contiguous; fully overwritten */
+    float* positions;
+    float* scales;
+    float* rotations;
+    float* density_r;
+    float* density_i;
+} gsv_grads;
+
+/* ---- library ---------------------------------------------------------- */
+
+GSV_API int gsv_abi_version(void);
+GSV_API const char* gsv_status_string(int status);
+/* Text of the last CUDA failure seen by this thread (GSV_ERR_CUDA). */
+GSV_API const char* gsv_last_error(void);
+/* Number of tiles, ceil(d/ts)*ceil(h/ts)*ceil(w/ts); -1 for an invalid shape. */
+GSV_API int64_t gsv_num_tiles(gsv_shape shape);
+
+/* ---- workspace sizing ------------------------------------------------- */
+
+/* Per-Gaussian / per-tile workspace (records, boxes, offsets, tile ranges,
+ * gradient accumulators, status word). */
+GSV_API size_t gsv_gauss_workspace_bytes(int64_t n, gsv_shape shape);
+/* Per-pair workspace for `capacity` pairs (sort keys/values, sort scratch,
+ * and the per-pair partials of the deterministic backward when
+ * `flags & GSV_BACKWARD_DETERMINISTIC`). */
+GSV_API size_t gsv_pair_workspace_bytes(int64_t capacity, gsv_shape shape, int flags);
+
+/* ---- fused native path ------------------------------------------------ */
+
+/* Preprocess every Gaussian (center, quadratic form, 3-sigma box), count its
+ * tiles and scan the counts.  If `total_pairs_host` is non-NULL the pair
+ * total is copied back and the stream is SYNCHRONISED (the reference's
+ * `.item()` at tile_voxelizer.py:118); pass NULL to stay asynchronous. */
+GSV_API int gsv_prepare(const gsv_params* params, gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
+                int64_t* total_pairs_host, void* stream);
+
+/* Emit (tile, Gaussian) pairs, radix-sort them by tile (stable: ascending
+ * Gaussian id within a tile) and build the per-tile ranges.  If the pair
+ * total exceeds `capacity` only `capacity` pairs are kept and
+ * GSV_FLAG_CAPACITY_OVERFLOW is latched. */
+GSV_API int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+            int64_t capacity, void* stream);
+
+/* Pointers to the tile ranges (int32 [T,2], empty tiles (0,0)) and the
+ * sorted pair ids (int32 [capacity]) held inside the workspaces. */
+GSV_API int gsv_bin_views(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, int64_t capacity,
+                  int32_t** tile_ranges, int32_t** pair_ids);
+
+/* Read the pair total and latched flags (SYNCHRONISES the stream). */
+GSV_API int gsv_read_status(gsv_shape shape, int64_t n, const void* ws_gauss, int64_t* total_pairs,
+                    int32_t* flags, void* stream);
+
+/* volume: complex64 [d*h*w], fully overwritten (tiles without Gaussians
+ * are written as zeros). */
+GSV_API int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,
+                int64_t capacity, float* volume, void* stream);
+
+/* grad_volume: complex64 [d*h*w] (dL/dRe, dL/dIm).  Writes dL/d(positions,
+ * scales, rotations, density_r, density_i).  `flags`: GSV_BACKWARD_*. */
+GSV_API int gsv_backward(const gsv_params* params, gsv_shape shape, void* ws_gauss, void* ws_pairs,
+                 int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
+                 void* stream);
+
+/* ---- reference-compatible binning ------------------------------------ */
+
+/* build_tile_pairs(center_vox [n,3], radius_vox [n]) part 1: box + count +
+ * scan.  Same synchronisation rule as gsv_prepare. */
+GSV_API int gsv_build_tile_pairs_count(const float* center_vox, const float* radius_vox, int64_t n,
+                               gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
+                               int64_t* total_pairs_host, void* stream);
+/* Part 2: writes tile_ranges int32 [T,2] and pair_ids int32 [capacity]
+ * (capacity >= the pair total from part 1) exactly as the reference lays
+ * them out, with ascending Gaussian id inside each tile. */
+GSV_API int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs,
+                              size_t ws_pairs_bytes, int64_t capacity, int32_t* tile_ranges,
+                              int32_t* pair_ids, void* stream);
+
+/* ---- reference-compatible kernels (the pybind forward/backward) ------- */
+
+/* centers [n,3] voxel units, cov_inv [n,3,3] normalised units (symmetric;
+ * the symmetric part is used), density_r/i [n], tile_ranges [T,2],
+ * pair_ids [P], half_shape [3] (device).  vol_r/vol_i [d*h*w] are fully
+ * overwritten. */
+GSV_API int gsv_tile_forward(const float* centers, const float* cov_inv, const float* density_r,
+                     const float* density_i, const int32_t* tile_ranges, const int32_t* pair_ids,
+                     const float* half_shape, int64_t n, int64_t num_tiles, int32_t tile_size,
+                     int32_t d, int32_t h, int32_t w, float* vol_r, float* vol_i, void* stream);
+
+/* Gradients w.r.t. centers [n,3], cov_inv [n,3,3] (symmetric), density_r,
+ * density_i [n]; outputs are zeroed by the callee, then accumulated. */
+GSV_API int gsv_tile_backward(const float* centers, const float* cov_inv, const float* density_r,
+                      const float* density_i, const int32_t* tile_ranges, const int32_t* pair_ids,
+                      const float* half_shape, const float* grad_vol_r, const float* grad_vol_i,
+                      int64_t n, int64_t num_tiles, int32_t tile_size, int32_t d, int32_t h,
+                      int32_t w, float* grad_centers, float* grad_cov_inv, float* grad_den_r,
+                      float* grad_den_i, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSV_H_ */

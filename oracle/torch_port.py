@@ -1,0 +1,75 @@
+"""PyTorch-CPU port of the reference's own CPU voxelizer path -- TEST / BASELINE
+INFRASTRUCTURE (bench.py's CPU-baseline leg and its ``--impl reference`` arm).
+
+It restates, in FP32 torch on the host cores, what the reference runs when
+its CUDA extension is unavailable (3DGS/3dgsVC/gaussian/tile_voxelizer.py):
+the torch preprocess (:282-290, :77-84), then for every non-empty tile a
+dense (voxels x listed Gaussians) evaluation -- distance normalised by the
+half shape, Mahalanobis form via einsum, exp(-m/2) masked by m <= 9,
+weighted density sum, scatter into the complex volume (:210-244) -- and
+autograd for the backward.  The reference module itself cannot be shipped
+with this repository, so this port is what the CPU baseline times.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import torch
+
+
+def _rotation(q: torch.Tensor) -> torch.Tensor:
+    q = q / (q.norm(dim=-1, keepdim=True) + 1e-8)
+    w, x, y, z = q.unbind(-1)
+    return torch.stack([
+        torch.stack([1 - 2 * y * y - 2 * z * z, 2 * x * y - 2 * z * w, 2 * x * z + 2 * y * w], -1),
+        torch.stack([2 * x * y + 2 * z * w, 1 - 2 * x * x - 2 * z * z, 2 * y * z - 2 * x * w], -1),
+        torch.stack([2 * x * z - 2 * y * w, 2 * y * z + 2 * x * w, 1 - 2 * x * x - 2 * y * y], -1),
+    ], -2)
+
+
+def preprocess(positions, scales, rotations, shape):
+    shape_t = torch.tensor(shape, dtype=torch.float32)
+    half = shape_t * 0.5
+    center = (positions + 1.0) * 0.5 * shape_t - 0.5
+    T = _rotation(rotations) * torch.reciprocal(scales + 1e-8).unsqueeze(1)
+    return center, T @ T.transpose(1, 2), half
+
+
+def tile_forward(center, cov_inv, density, half, tile_ranges, pair_ids, shape, tile_size, tiles):
+    """Complex64 flat volume from the listed tiles (dense per-tile evaluation)."""
+    d, h, w = shape
+    n_th, n_tw = math.ceil(h / tile_size), math.ceil(w / tile_size)
+    vol = torch.zeros(d * h * w, dtype=torch.complex64)
+    for t in tiles:
+        s, e = int(tile_ranges[t, 0]), int(tile_ranges[t, 1])
+        if s >= e:
+            continue
+        gids = torch.from_numpy(pair_ids[s:e].astype(np.int64))
+        td, rem = divmod(int(t), n_th * n_tw)
+        th, tw = divmod(rem, n_tw)
+        rd = torch.arange(td * tile_size, min(td * tile_size + tile_size, d), dtype=torch.float32)
+        rh = torch.arange(th * tile_size, min(th * tile_size + tile_size, h), dtype=torch.float32)
+        rw = torch.arange(tw * tile_size, min(tw * tile_size + tile_size, w), dtype=torch.float32)
+        gd, gh, gw = torch.meshgrid(rd, rh, rw, indexing="ij")
+        vox = torch.stack([gd, gh, gw], -1).reshape(-1, 3)
+        diff = (vox.unsqueeze(1) - center[gids].unsqueeze(0)) / half
+        mahal = torch.einsum("vgi,gij,vgj->vg", diff, cov_inv[gids], diff)
+        wgt = torch.exp(-0.5 * mahal) * (mahal <= 9.0).float()
+        contrib = (wgt.to(torch.complex64) * density[gids].unsqueeze(0)).sum(1)
+        flat = (gd.reshape(-1).long() * h + gh.reshape(-1).long()) * w + gw.reshape(-1).long()
+        vol = vol.index_add(0, flat, contrib)
+    return vol
+
+
+def time_fwd_bwd(params, shape, tile_size, tile_ranges, pair_ids, grad_vol, tiles):
+    """Forward + autograd backward over `tiles`; returns seconds."""
+    pos, scl, rot, dr, di = (torch.tensor(np.asarray(x), dtype=torch.float32).requires_grad_(True) for x in params)
+    g = torch.tensor(np.asarray(grad_vol).reshape(-1), dtype=torch.complex64)
+    t0 = time.perf_counter()
+    center, cov_inv, half = preprocess(pos, scl, rot, shape)
+    vol = tile_forward(center, cov_inv, torch.complex(dr, di), half, tile_ranges, pair_ids, shape, tile_size, tiles)
+    loss = (vol.real * g.real + vol.imag * g.imag).sum()
+    loss.backward()
+    return time.perf_counter() - t0
