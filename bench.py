@@ -86,6 +86,13 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # start timing only once the sampler is producing rows
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
@@ -126,7 +133,7 @@ def count_library_launches(fn, dev):
         return None, [f"profiler unavailable: {exc}"]
 
 
-def cpu_baseline(gs, gv, shape, seconds=12.0):
+def cpu_baseline(gs, gv, shape, seconds=12.0, warm=True):
     """CPU port of the reference's CPU path on a bounded random sample of
     tiles of the same workload, all host threads."""
     from oracle import oracle as O
@@ -141,8 +148,9 @@ def cpu_baseline(gs, gv, shape, seconds=12.0):
     nt = tr.shape[0]
     order = np.random.default_rng(0).permutation(nt)
     per_tile = (tr[:, 1] - tr[:, 0]).astype(np.int64) * TILE ** 3  # interior tiles (shape divisible by 8)
-    torch_port.time_fwd_bwd(p, shape, TILE, tr, pid, gv.numpy(), order[:2])  # warm-up
-    done, evals, t_total, chunk = 0, 0, 0.0, 8
+    if warm:
+        torch_port.time_fwd_bwd(p, shape, TILE, tr, pid, gv.numpy(), order[:2])
+    done, evals, t_total, chunk = 0, 0, 0.0, 1
     while t_total < seconds and done < nt:
         tiles = order[done:done + chunk]
         t_total += torch_port.time_fwd_bwd(p, shape, TILE, tr, pid, gv.numpy(), tiles)
@@ -162,9 +170,11 @@ def run_reference(args, rank, world):
     gs, gv = make_inputs(name)
     shape = WORKLOADS[name]["shape"]
     vals, times = [], []
-    for i in range(args.warmup + args.steps):
-        b = cpu_baseline(gs, gv, shape, seconds=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
-        if i >= args.warmup:
+    steps, warm = args.steps, args.warmup
+    # each step is a bounded sample so the whole run stays near 90 s of CPU work
+    for i in range(warm + steps):
+        b = cpu_baseline(gs, gv, shape, seconds=max(0.02, 90.0 / (steps + warm)), warm=(i == 0))
+        if i >= warm:
             vals.append(b["value"])
             times.append(b["seconds"])
     v = statistics.mean(vals)
@@ -238,7 +248,7 @@ def run_ours(args, rank, world, dist):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
-    n_launch, kernel_names = count_library_launches(step, dev)
+    n_launch, kernel_names = (None, []) if args.no_launch_count else count_library_launches(step, dev)
 
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     cur = torch.cuda.current_stream(dev)
@@ -349,12 +359,13 @@ def run_ours(args, rank, world, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mri128x128x96_n50k")
     ap.add_argument("--deterministic", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-launch-count", action="store_true", help="skip the CUDA activity trace (under ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
