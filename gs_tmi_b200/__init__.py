@@ -3,7 +3,7 @@
 Drop-in for the reference ``gaussian.TileVoxelizer`` plugin: same
 constructor / forward signature and autograd behaviour, backed by the C ABI
 in ``include/gsv.h`` (``lib/libgsv_b200.so``, built with
-``python -m gs_tmi_b200.build``).  Importing this package fails loudly when
+``python gs_tmi_b200/build.py``).  Importing this package fails loudly when
 the library is missing: there is no CPU path.
 """
 from .tile_voxelizer import (  # noqa: F401

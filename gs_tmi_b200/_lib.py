@@ -71,7 +71,7 @@ def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"{LIB_PATH} is missing: build the sm_100a voxelizer library with "
-            "`python -m gs_tmi_b200.build` (this package has no CPU fallback)")
+            "`python gs_tmi_b200/build.py` (this package has no CPU fallback)")
     lib = ctypes.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

@@ -1,7 +1,7 @@
 """Build the sm_100a voxelizer library in-tree: gs_tmi_b200/lib/libgsv_b200.so.
 
-    python -m gs_tmi_b200.build          # incremental
-    python -m gs_tmi_b200.build --force  # rebuild everything
+    python gs_tmi_b200/build.py          # incremental
+    python gs_tmi_b200/build.py --force  # rebuild everything
 
 Each ``csrc/*.cu`` is compiled to an object with nvcc in parallel and the
 objects are linked into one shared library with the CUDA runtime linked
