@@ -160,6 +160,25 @@ GSV_API int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss
                               size_t ws_pairs_bytes, int64_t capacity, int32_t* tile_ranges,
                               int32_t* pair_ids, void* stream);
 
+/* No counterpart in the reference.  Binning for callers that cannot allocate
+ * device memory -- their GPU memory belongs to another allocator (a framework
+ * that reserves the device up front, a process under a hard memory cap) or
+ * they run on a path with a fixed memory plan.  Same outputs as
+ * gsv_build_tile_pairs_count + gsv_build_tile_pairs_fill, but every scratch
+ * buffer comes from one static device array of about 41 MiB that each GPU
+ * loading this library holds until the process exits; the caller passes only
+ * inputs and outputs.  Limits: n <= 262,144 Gaussians (else
+ * GSV_ERR_INVALID_ARGUMENT) and at most 2,097,152 pairs (else
+ * GSV_ERR_CAPACITY; GSV_ERR_CAPACITY also when the pair total exceeds
+ * `pair_capacity`).  `*total_pairs` always receives the pair total; the call
+ * synchronises `stream` once to read it.  The first call on a device (with
+ * that device current) looks up the array's device address; make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them. */
+GSV_API int gsv_build_tile_pairs_noalloc(const float* center_vox, const float* radius_vox, int64_t n,
+                                         gsv_shape shape, int32_t* tile_ranges, int32_t* pair_ids,
+                                         int64_t pair_capacity, int64_t* total_pairs, void* stream);
+
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 
 /* centers [n,3] voxel units, cov_inv [n,3,3] normalised units (symmetric;
