@@ -30,11 +30,16 @@ def _rotation(q: torch.Tensor) -> torch.Tensor:
 
 
 def preprocess(positions, scales, rotations, shape):
-    shape_t = torch.tensor(shape, dtype=torch.float32)
+    """center_vox, cov_inv, half_shape (tile_voxelizer.py:282-290)."""
+    shape_t = torch.tensor(shape, dtype=torch.float32, device=positions.device)
     half = shape_t * 0.5
     center = (positions + 1.0) * 0.5 * shape_t - 0.5
     T = _rotation(rotations) * torch.reciprocal(scales + 1e-8).unsqueeze(1)
     return center, T @ T.transpose(1, 2), half
+
+
+def radius_vox(scales, half):
+    return (scales * half).max(dim=-1)[0] * 3.0
 
 
 def tile_forward(center, cov_inv, density, half, tile_ranges, pair_ids, shape, tile_size, tiles):
@@ -73,3 +78,48 @@ def time_fwd_bwd(params, shape, tile_size, tile_ranges, pair_ids, grad_vol, tile
     loss = (vol.real * g.real + vol.imag * g.imag).sum()
     loss.backward()
     return time.perf_counter() - t0
+
+
+def build_tile_pairs_torch(center_vox, radius_vox, shape, tile_size):
+    """Torch restatement of the reference's binning (tile_voxelizer.py:87-162),
+    runnable on CPU or GPU; includes the reference's host sync on the pair
+    total.  Used to time the reference's full step on the GPU."""
+    d, h, w = shape
+    dev = center_vox.device
+    n = center_vox.shape[0]
+    ntd, nth, ntw = (math.ceil(s / tile_size) for s in shape)
+    r3 = radius_vox.unsqueeze(1).expand(-1, 3)
+    lo = (center_vox - r3).floor().int()
+    hi = (center_vox + r3).ceil().int()
+    size = torch.tensor([d, h, w], device=dev, dtype=torch.int32)
+    nt = torch.tensor([ntd, nth, ntw], device=dev, dtype=torch.int32)
+    lo = torch.minimum(torch.clamp(lo, min=0), size - 1)
+    hi = torch.minimum(torch.clamp(hi, min=0), size - 1)
+    tmin = torch.minimum(torch.clamp(lo // tile_size, min=0), nt - 1)
+    tmax = torch.minimum(torch.clamp(hi // tile_size, min=0), nt - 1)
+    n_per = tmax - tmin + 1
+    cnt = n_per[:, 0] * n_per[:, 1] * n_per[:, 2]
+    total = int(cnt.sum().item())
+    ranges = torch.zeros(ntd * nth * ntw, 2, dtype=torch.int32, device=dev)
+    if total == 0:
+        return ranges, torch.zeros(0, dtype=torch.int32, device=dev)
+    gid = torch.repeat_interleave(torch.arange(n, device=dev, dtype=torch.int32), cnt)
+    start = torch.cumsum(cnt, 0) - cnt
+    local = torch.arange(total, device=dev, dtype=torch.int64) - torch.repeat_interleave(start, cnt)
+    nh = torch.repeat_interleave(n_per[:, 1], cnt)
+    nw = torch.repeat_interleave(n_per[:, 2], cnt)
+    ld, lr = local // (nh * nw), local % (nh * nw)
+    lh, lw = lr // nw, lr % nw
+    td = torch.repeat_interleave(tmin[:, 0], cnt) + ld.int()
+    th = torch.repeat_interleave(tmin[:, 1], cnt) + lh.int()
+    tw = torch.repeat_interleave(tmin[:, 2], cnt) + lw.int()
+    tile = (td * nth * ntw + th * ntw + tw).int()
+    order = torch.argsort(tile, stable=True)
+    tile_s, gid_s = tile[order], gid[order]
+    change = torch.ones(total, dtype=torch.bool, device=dev)
+    change[1:] = tile_s[1:] != tile_s[:-1]
+    pos = torch.nonzero(change, as_tuple=True)[0]
+    ends = torch.cat([pos[1:], torch.tensor([total], device=dev)])
+    ranges[tile_s[pos].long(), 0] = pos.int()
+    ranges[tile_s[pos].long(), 1] = ends.int()
+    return ranges, gid_s
