@@ -57,12 +57,16 @@ SIGNATURES = {
     "gsv_prepare": (ctypes.c_int, [_P, _S, _vp, _sz, _i64p, _vp]),
     "gsv_bin": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp]),
     "gsv_bin_views": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "gsv_status_views": (ctypes.c_int, [_S, _i64, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsv_read_status": (ctypes.c_int, [_S, _i64, _vp, _i64p, _i32p, _vp]),
     "gsv_forward": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, _vp, _vp]),
     "gsv_backward": (ctypes.c_int, [_P, _S, _vp, _vp, _i64, _vp, _G, ctypes.c_int, _vp]),
     "gsv_build_tile_pairs_count": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _sz, _i64p, _vp]),
     "gsv_build_tile_pairs_fill": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp, _vp, _vp]),
     "gsv_build_tile_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _vp, _i64, _i64p, _vp]),
+    "gsv_mlp_gemm": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
+                                    ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                    _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),
 }

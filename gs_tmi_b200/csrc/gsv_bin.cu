@@ -411,6 +411,15 @@ int gsv_bin_views(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, in
     return GSV_OK;
 }
 
+int gsv_status_views(gsv_shape shape, int64_t n, void* ws_gauss, int32_t** flags, int64_t** total_pairs) {
+    ShapeInfo si = shape_info(shape);
+    if (!si.ok || n < 0 || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
+    const GaussLayout L = gauss_layout(n, si);
+    if (flags) *flags = &at<Status>(ws_gauss, L.status)->flags;
+    if (total_pairs) *total_pairs = at<int64_t>(ws_gauss, L.offsets) + n;
+    return GSV_OK;
+}
+
 int gsv_read_status(gsv_shape shape, int64_t n, const void* ws_gauss, int64_t* total_pairs,
                     int32_t* flags, void* stream) {
     ShapeInfo si = shape_info(shape);

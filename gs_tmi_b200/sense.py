@@ -1,0 +1,511 @@
+"""The SENSE data-consistency loop that calls the voxelizer (plain 3DGSMR fit).
+
+A compact restatement of the reference trainer's plain method, used as the
+caller of the voxelizer for reconstruction runs, parity runs against the
+reference kernels and the warm-start evaluation.  Reference (V = 3DGS/3dgsVC):
+
+* loss (``V/trainers/trainer.py:256-283``, ``V/losses/losses.py:18-26``):
+  || mask * fft3c(S x) - y ||^2 + tv_weight * TV(|x|)
+* optimiser (``trainer.py:167-183``, ``V/gaussian/gaussian_model.py:76-83``):
+  Adam with per-tensor learning rates, ExponentialLR(gamma), grad-norm clip
+  (``trainer.py:426-439``)
+* adaptive density control (``trainer.py:294-352``,
+  ``gaussian_model.py:85-222``): split (two children drawn around the parent,
+  scales / 1.6, density x 0.5), clone (density halved and duplicated), prune
+  (|rho| < opacity threshold or max scale > limit), Adam moments transplanted
+  for surviving rows (``trainer.py:355-424``)
+* evaluation (``trainer.py:237-243``, ``V/metrics/metrics.py:70-77``):
+  hard data consistency, then magnitude NMSE; SSIM follows the published
+  definition (Wang et al. 2004) with a uniform 7^3 window, K1=0.01, K2=0.03,
+  sample covariance.
+
+The voxelizer is any callable (positions, scales, rotations, density) ->
+complex64 volume; the default is this package's ``TileVoxelizer``.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional
+
+import torch
+import torch.nn as nn
+import torch.nn.functional as F
+
+from .synthetic import GaussianSet, MRICase, fft3c, ifft3c
+
+
+@dataclass
+class FitConfig:
+    iterations: int = 2000
+    position_lr: float = 1e-3
+    scale_lr: float = 5e-3
+    rotation_lr: float = 1e-3
+    density_lr: float = 1e-2
+    gamma: float = 0.999
+    max_grad_norm: float = 1.0
+    tv_weight: float = 0.1
+    densify_from: int = 100
+    densify_every: int = 100
+    densify_until: int = 2500
+    grad_threshold: float = 0.01
+    scale_threshold: float = 0.01
+    opacity_threshold: float = 0.01
+    max_scale: float = 0.5
+    max_points: int = 500_000
+    use_cloning: bool = True
+    tile_size: int = 8
+    deterministic: bool = False
+    eval_every: int = 100
+    seed: int = 0
+
+
+# ---------------------------------------------------------------------------
+# metrics / losses
+# ---------------------------------------------------------------------------
+
+def magnitude_tv(vol: torch.Tensor) -> torch.Tensor:
+    m = vol.abs()
+    return ((m[1:] - m[:-1]).abs().sum() + (m[:, 1:] - m[:, :-1]).abs().sum()
+            + (m[:, :, 1:] - m[:, :, :-1]).abs().sum())
+
+
+def nmse(pred: torch.Tensor, target: torch.Tensor) -> float:
+    p, t = pred.abs().double(), target.abs().double()
+    den = float((t * t).sum())
+    return float(((p - t) ** 2).sum()) / den if den > 0 else float("inf")
+
+
+def psnr(pred: torch.Tensor, target: torch.Tensor) -> float:
+    p, t = pred.abs().double(), target.abs().double()
+    mse = float(((p - t) ** 2).mean())
+    peak = float(t.max())
+    return 10 * math.log10(peak * peak / mse) if mse > 0 else float("inf")
+
+
+def ssim3d(pred: torch.Tensor, target: torch.Tensor, data_range: Optional[float] = None, win: int = 7) -> float:
+    x = pred.abs().double()[None, None]
+    y = target.abs().double()[None, None]
+    if data_range is None:
+        data_range = float(y.max() - y.min()) or 1.0
+    c1, c2 = (0.01 * data_range) ** 2, (0.03 * data_range) ** 2
+    n = win ** 3
+    mu = lambda a: F.avg_pool3d(a, win, stride=1)
+    mx, my = mu(x), mu(y)
+    cov = n / (n - 1)
+    sxx = (mu(x * x) - mx * mx) * cov
+    syy = (mu(y * y) - my * my) * cov
+    sxy = (mu(x * y) - mx * my) * cov
+    s = ((2 * mx * my + c1) * (2 * sxy + c2)) / ((mx * mx + my * my + c1) * (sxx + syy + c2))
+    return float(s.mean())
+
+
+def hard_data_consistency(vol, S, mask, ku):
+    """Replace the measured k-space samples (trainer.py:237-243)."""
+    k = fft3c(vol.unsqueeze(0) * S)
+    k = k * (1.0 - mask.unsqueeze(0)) + ku
+    return (torch.conj(S) * ifft3c(k)).sum(0)
+
+
+# ---------------------------------------------------------------------------
+# parameters, optimiser, density control
+# ---------------------------------------------------------------------------
+
+class GaussianParams(nn.Module):
+    """positions [N,3], log-scales [N,3], rotations [N,4], density re/im [N]
+    as nn.Parameters (the layout of gaussian_model.py:38-68)."""
+
+    def __init__(self, init: GaussianSet, device):
+        super().__init__()
+        self.positions = nn.Parameter(init.positions.to(device).clone())
+        self.log_scales = nn.Parameter(torch.log(init.scales.to(device).clamp_min(1e-8)))
+        self.rotations = nn.Parameter(init.rotations.to(device).clone())
+        self.density_r = nn.Parameter(init.density_r.to(device).clone())
+        self.density_i = nn.Parameter(init.density_i.to(device).clone())
+
+    @property
+    def n(self) -> int:
+        return int(self.positions.shape[0])
+
+    def tensors(self):
+        return [self.positions, self.log_scales, self.rotations, self.density_r, self.density_i]
+
+    def replace(self, new: List[torch.Tensor]):
+        for name, t in zip(("positions", "log_scales", "rotations", "density_r", "density_i"), new):
+            setattr(self, name, nn.Parameter(t.detach().contiguous()))
+
+    def snapshot(self) -> GaussianSet:
+        return GaussianSet(self.positions.detach().clone(), torch.exp(self.log_scales.detach()),
+                           self.rotations.detach().clone(), self.density_r.detach().clone(),
+                           self.density_i.detach().clone())
+
+
+def make_optimizer(p: GaussianParams, cfg: FitConfig, lrs=None, fused: Optional[bool] = None,
+                   capturable: bool = False):
+    lr = lrs or [cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr, cfg.density_lr]
+    groups = [{"params": [t], "lr": l} for t, l in zip(p.tensors(), lr)]
+    kw = {}
+    if fused is None:
+        fused = p.positions.is_cuda
+    if fused:
+        kw["fused"] = True
+    if capturable:
+        kw["capturable"] = True
+    return torch.optim.Adam(groups, **kw)
+
+
+def transplant(old_opt, new_opt, keep: torch.Tensor, n_new: int):
+    """Adam moments of surviving rows move to the new tensors; appended rows
+    start at zero (trainer.py:355-389)."""
+    for og, ng in zip(old_opt.param_groups, new_opt.param_groups):
+        op, np_ = og["params"][0], ng["params"][0]
+        st = old_opt.state.get(op)
+        if not st or "exp_avg" not in st:
+            continue
+        new_state = {}
+        for key in ("exp_avg", "exp_avg_sq"):
+            kept = st[key][keep]
+            pad = np_.shape[0] - kept.shape[0]
+            if pad > 0:
+                kept = torch.cat([kept, kept.new_zeros((pad,) + tuple(kept.shape[1:]))], 0)
+            new_state[key] = kept.contiguous()
+        new_state["step"] = st["step"].clone() if torch.is_tensor(st["step"]) else st["step"]
+        new_opt.state[np_] = new_state
+
+
+@torch.no_grad()
+def density_control(p: GaussianParams, pos_grad: torch.Tensor, cfg: FitConfig, gen: torch.Generator,
+                    on_event: Callable[[torch.Tensor], None]):
+    """Split, clone, prune (trainer.py:294-352, gaussian_model.py:85-186).
+    After every change of the parameter tensors ``on_event(keep_mask)`` runs
+    (the optimiser rebuild of trainer.py:391-424); returns the event count."""
+    events = 0
+    if p.n >= cfg.max_points:
+        return events
+    gnorm = pos_grad.norm(dim=-1)
+    scales = torch.exp(p.log_scales)
+    smax = scales.max(-1)[0]
+    high = gnorm > cfg.grad_threshold
+    split = high & (smax > cfg.scale_threshold)
+    n_split = int(split.sum())
+    did_split_branch = False
+    if n_split > 0 and p.n + n_split <= cfg.max_points:
+        did_split_branch = True
+        par_pos = p.positions[split]
+        par_s = scales[split]
+        na = torch.randn(par_pos.shape, device=par_pos.device, generator=gen) * par_s * 0.5
+        nb = torch.randn(par_pos.shape, device=par_pos.device, generator=gen) * par_s * 0.5
+        keep = ~split
+        new = [torch.cat([p.positions[keep], par_pos + na, par_pos + nb]),
+               torch.cat([p.log_scales[keep], torch.log(par_s / 1.6 + 1e-8).repeat(2, 1)]),
+               torch.cat([p.rotations[keep], p.rotations[split].repeat(2, 1)]),
+               torch.cat([p.density_r[keep], (p.density_r[split] * 0.5).repeat(2)]),
+               torch.cat([p.density_i[keep], (p.density_i[split] * 0.5).repeat(2)])]
+        p.replace(new)
+        on_event(keep)
+        events += 1
+    if cfg.use_cloning and not did_split_branch:
+        clone = high & (smax <= cfg.scale_threshold)
+        n_clone = int(clone.sum())
+        if n_clone > 0 and p.n + n_clone <= cfg.max_points:
+            dr = p.density_r.detach().clone()
+            di = p.density_i.detach().clone()
+            dr[clone] *= 0.5
+            di[clone] *= 0.5
+            keep = torch.ones(p.n, dtype=torch.bool, device=dr.device)
+            new = [torch.cat([p.positions, p.positions[clone]]),
+                   torch.cat([p.log_scales, torch.log(scales[clone] + 1e-8)]),
+                   torch.cat([p.rotations, p.rotations[clone]]),
+                   torch.cat([dr, dr[clone]]), torch.cat([di, di[clone]])]
+            p.replace(new)
+            on_event(keep)
+            events += 1
+    scales = torch.exp(p.log_scales)
+    smax = scales.max(-1)[0]
+    mag = torch.sqrt(p.density_r * p.density_r + p.density_i * p.density_i)
+    prune = (mag < cfg.opacity_threshold) | (smax > cfg.max_scale)
+    keep = ~prune
+    if int(keep.sum()) >= 100 and int(prune.sum()) > 0:
+        p.replace([t[keep] for t in p.tensors()])
+        on_event(keep)
+        events += 1
+    return events
+
+
+# ---------------------------------------------------------------------------
+# the fit
+# ---------------------------------------------------------------------------
+
+def _sync(dev: torch.device):
+    if dev.type == "cuda":
+        torch.cuda.synchronize(dev)
+
+@dataclass
+class FitResult:
+    params: GaussianParams
+    history: List[Dict] = field(default_factory=list)
+    seconds: float = 0.0
+    final_nmse: float = float("nan")
+    final_ssim: float = float("nan")
+    final_psnr: float = float("nan")
+
+
+def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Callable] = None,
+        device="cuda:0", stop_nmse: Optional[float] = None, log: Optional[Callable] = None,
+        eval_ssim: bool = True) -> FitResult:
+    """Plain 3DGSMR fit of `case` from `init`.  Wall time excludes the
+    evaluations; `stop_nmse` ends the fit at the first evaluation at or below
+    that hard-DC NMSE (time-to-NMSE runs)."""
+    dev = torch.device(device)
+    shape = tuple(case.ground_truth.shape)
+    if voxelizer is None:
+        from .tile_voxelizer import TileVoxelizer
+
+        voxelizer = TileVoxelizer(shape, tile_size=cfg.tile_size, device=str(dev), deterministic=cfg.deterministic)
+    S = case.sensitivity_maps.to(dev)
+    mask = case.mask.to(dev)
+    ku = case.kspace_undersampled.to(dev)
+    gt = case.ground_truth.to(dev)
+    p = GaussianParams(init, dev)
+    opt = make_optimizer(p, cfg)
+    lrs = [cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr, cfg.density_lr]
+    gen = torch.Generator(device=dev).manual_seed(cfg.seed)
+    res = FitResult(params=p)
+    mask_c = mask.unsqueeze(0)
+    skip_sched = False
+    wall = 0.0
+    _sync(dev)
+    t0 = time.perf_counter()
+    for it in range(cfg.iterations):
+        opt.zero_grad(set_to_none=True)
+        vol = voxelizer(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
+        if isinstance(vol, tuple):
+            vol = torch.complex(vol[0], vol[1])
+        diff = fft3c(vol.unsqueeze(0) * S) * mask_c - ku
+        loss = diff.real.square().sum() + diff.imag.square().sum()
+        if cfg.tv_weight > 0:
+            loss = loss + cfg.tv_weight * magnitude_tv(vol)
+        loss.backward()
+        pos_grad = p.positions.grad.detach().clone()
+        if cfg.max_grad_norm > 0:
+            torch.nn.utils.clip_grad_norm_(p.tensors(), cfg.max_grad_norm)
+        opt.step()
+        if (cfg.densify_from <= it <= cfg.densify_until and it % cfg.densify_every == 0):
+            holder = [opt]
+            lrs = [g["lr"] for g in opt.param_groups]
+
+            def rebuild(keep, holder=holder, lrs=lrs):
+                new_opt = make_optimizer(p, cfg, lrs)
+                transplant(holder[0], new_opt, keep, p.n)
+                holder[0] = new_opt
+
+            if density_control(p, pos_grad, cfg, gen, rebuild):
+                opt = holder[0]
+                skip_sched = True
+        if skip_sched:
+            skip_sched = False
+        else:
+            for g in opt.param_groups:
+                g["lr"] *= cfg.gamma
+        last = it == cfg.iterations - 1
+        if (it % cfg.eval_every == 0) or last:
+            _sync(dev)
+            wall += time.perf_counter() - t0
+            with torch.no_grad():
+                v = voxelizer(p.positions, torch.exp(p.log_scales), p.rotations,
+                              torch.complex(p.density_r, p.density_i))
+                if isinstance(v, tuple):
+                    v = torch.complex(v[0], v[1])
+                rec = hard_data_consistency(v, S, mask, ku)
+                e = nmse(rec, gt)
+            row = {"iteration": it, "loss": float(loss.detach()), "nmse": e, "n_points": p.n, "seconds": wall}
+            res.history.append(row)
+            if log:
+                log(row)
+            done = stop_nmse is not None and e <= stop_nmse
+            if last or done:
+                res.final_nmse = e
+                res.final_psnr = psnr(rec, gt)
+                if eval_ssim:
+                    res.final_ssim = ssim3d(rec, gt)
+                if done:
+                    break
+            _sync(dev)
+            t0 = time.perf_counter()
+    res.seconds = wall
+    return res
+
+
+# ---------------------------------------------------------------------------
+# the same fit with each iteration replayed from a CUDA graph
+# ---------------------------------------------------------------------------
+
+class _GraphedStep:
+    """One training iteration (voxelize -> coils -> FFT -> mask -> loss ->
+    backward -> clip -> Adam) captured in a CUDA graph for a fixed Gaussian
+    count.  The graph first snapshots parameters and Adam state, so an
+    iteration whose tile pairs overflowed the static capacity can be undone
+    and re-run with a larger capacity."""
+
+    def __init__(self, p, opt, vox, S, mask_c, ku, cfg, capacity):
+        self.p, self.opt, self.cfg = p, opt, cfg
+        self.svox = vox.static(p.n, capacity)
+        self.capacity = capacity
+        dev = p.positions.device
+        for t in p.tensors():
+            t.grad = torch.zeros_like(t)
+        self.pos_grad = torch.zeros_like(p.positions)
+        self.loss = torch.zeros((), device=dev)
+        self.flags_host = torch.zeros(1, dtype=torch.int32).pin_memory()
+        self.state_tensors = []
+        for t in p.tensors():
+            st = opt.state.get(t, {})
+            self.state_tensors += [st[k] for k in ("exp_avg", "exp_avg_sq", "step") if k in st]
+        self.live = p.tensors() + self.state_tensors
+        self.snap = [torch.empty_like(t) for t in self.live]
+        self.S, self.mask_c, self.ku = S, mask_c, ku
+        self.graph = None
+
+    def _body(self):
+        torch._foreach_copy_(self.snap, self.live)
+        for t in self.p.tensors():
+            t.grad.zero_()
+        p = self.p
+        vol = self.svox(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
+        diff = fft3c(vol.unsqueeze(0) * self.S) * self.mask_c - self.ku
+        loss = diff.real.square().sum() + diff.imag.square().sum()
+        if self.cfg.tv_weight > 0:
+            loss = loss + self.cfg.tv_weight * magnitude_tv(vol)
+        loss.backward()
+        self.pos_grad.copy_(p.positions.grad)
+        if self.cfg.max_grad_norm > 0:
+            torch.nn.utils.clip_grad_norm_(p.tensors(), self.cfg.max_grad_norm)
+        self.opt.step()
+        self.loss.copy_(loss.detach())
+        self.flags_host.copy_(self.svox.plan.flags_dev, non_blocking=True)
+
+    def eager(self):
+        """Run one real iteration outside the graph (also the capture warm-up)."""
+        dev = self.p.positions.device
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            self._body()
+        torch.cuda.current_stream(dev).wait_stream(side)
+
+    def capture(self):
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._body()
+
+    def replay(self):
+        self.graph.replay()
+
+    def overflowed(self) -> bool:
+        torch.cuda.current_stream(self.p.positions.device).synchronize()
+        return bool(int(self.flags_host[0]) & 1)
+
+    def undo(self):
+        torch._foreach_copy_(self.live, self.snap)
+
+
+def fit_graph(case: MRICase, init: GaussianSet, cfg: FitConfig, device="cuda:0", stop_nmse: Optional[float] = None,
+              log: Optional[Callable] = None, eval_ssim: bool = True, capacity_margin: float = 1.25,
+              stats: Optional[Dict] = None) -> FitResult:
+    """`fit` with every iteration replayed from a CUDA graph.  The graph is
+    (re)captured after the first iteration and after every density-control
+    change; the voxelizer inside runs on a fixed pair capacity (the current
+    pair count x `capacity_margin`), and an overflowing iteration is undone
+    and re-run after re-sizing."""
+    from .tile_voxelizer import TileVoxelizer
+
+    dev = torch.device(device)
+    shape = tuple(case.ground_truth.shape)
+    vox = TileVoxelizer(shape, tile_size=cfg.tile_size, device=str(dev), deterministic=cfg.deterministic)
+    S = case.sensitivity_maps.to(dev)
+    mask = case.mask.to(dev)
+    ku = case.kspace_undersampled.to(dev)
+    gt = case.ground_truth.to(dev)
+    mask_c = mask.unsqueeze(0)
+    p = GaussianParams(init, dev)
+    lrs = [torch.tensor(v, device=dev) for v in (cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr,
+                                                   cfg.density_lr)]
+    opt = make_optimizer(p, cfg, lrs=lrs, capturable=True)
+    gen = torch.Generator(device=dev).manual_seed(cfg.seed)
+    res = FitResult(params=p)
+    st = stats if stats is not None else {}
+    st.setdefault("captures", 0)
+    st.setdefault("overflows", 0)
+
+    def new_step():
+        cap = int(vox.count_pairs(p.positions.detach(), torch.exp(p.log_scales.detach())) * capacity_margin) + 4096
+        return _GraphedStep(p, opt, vox, S, mask_c, ku, cfg, cap)
+
+    step = None
+    wall = 0.0
+    _sync(dev)
+    t0 = time.perf_counter()
+    for it in range(cfg.iterations):
+        while True:
+            if step is None or step.graph is None:
+                if step is None:
+                    step = new_step()
+                step.eager()
+                if step.overflowed():
+                    step.undo()
+                    st["overflows"] += 1
+                    step = _GraphedStep(p, opt, vox, S, mask_c, ku, cfg, step.capacity * 2)
+                    continue
+                step.capture()
+                st["captures"] += 1
+                break
+            step.replay()
+            if not step.overflowed():
+                break
+            step.undo()
+            st["overflows"] += 1
+            step = _GraphedStep(p, opt, vox, S, mask_c, ku, cfg, step.capacity * 2)
+            step.graph = None
+        skip_sched = False
+        if cfg.densify_from <= it <= cfg.densify_until and it % cfg.densify_every == 0:
+            holder = [opt]
+            cur_lrs = [g["lr"] for g in opt.param_groups]
+
+            def rebuild(keep, holder=holder, cur_lrs=cur_lrs):
+                new_opt = make_optimizer(p, cfg, cur_lrs, capturable=True)
+                transplant(holder[0], new_opt, keep, p.n)
+                holder[0] = new_opt
+
+            if density_control(p, step.pos_grad, cfg, gen, rebuild):
+                opt = holder[0]
+                skip_sched = True
+                step = None
+        if not skip_sched:
+            torch._foreach_mul_(lrs, cfg.gamma)
+        last = it == cfg.iterations - 1
+        if (it % cfg.eval_every == 0) or last:
+            _sync(dev)
+            wall += time.perf_counter() - t0
+            with torch.no_grad():
+                v = vox(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
+                rec = hard_data_consistency(v, S, mask, ku)
+                e = nmse(rec, gt)
+            lossv = float(step.loss) if step is not None else float("nan")
+            row = {"iteration": it, "loss": lossv, "nmse": e, "n_points": p.n, "seconds": wall}
+            res.history.append(row)
+            if log:
+                log(row)
+            done = stop_nmse is not None and e <= stop_nmse
+            if last or done:
+                res.final_nmse = e
+                res.final_psnr = psnr(rec, gt)
+                if eval_ssim:
+                    res.final_ssim = ssim3d(rec, gt)
+                if done:
+                    break
+            _sync(dev)
+            t0 = time.perf_counter()
+    res.seconds = wall
+    res.params = p
+    return res

@@ -167,6 +167,56 @@ def backward_into(plan: BinPlan, params, grad_vol: torch.Tensor, outs) -> None:
                            _stream(plan.device)), "gsv_backward")
 
 
+class StaticPlan(BinPlan):
+    """Workspace preallocated for `n` Gaussians and a fixed pair capacity.
+    The voxelizer then makes no host synchronisation and no allocation of
+    its own, so a whole iteration can be captured in a CUDA graph.  Pairs
+    beyond the capacity are dropped and GSV_FLAG_CAPACITY_OVERFLOW is latched
+    in ``flags_dev`` (copy it out and check it after each replay)."""
+
+    def __init__(self, shape: GsvShape, n: int, device: torch.device, capacity: int, flags: int = 0):
+        super().__init__(shape, n, device, flags)
+        self.alloc_pairs(capacity)
+        fl, tot = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib.gsv_status_views(shape, n, _ptr(self.ws_gauss), ctypes.byref(fl), ctypes.byref(tot)),
+              "gsv_status_views")
+        base = self.ws_gauss.data_ptr()
+        self.flags_dev = self.ws_gauss[fl.value - base:fl.value - base + 4].view(torch.int32)
+        self.total_dev = self.ws_gauss[tot.value - base:tot.value - base + 8].view(torch.int64)
+
+
+class _VoxelizeStaticFn(torch.autograd.Function):
+    """Same math as _VoxelizeFn on a StaticPlan: no host sync, no workspace
+    allocation (CUDA-graph capturable)."""
+
+    @staticmethod
+    def forward(ctx, positions, scales, rotations, density_r, density_i, plan):
+        params = tuple(_f32(t) for t in (positions, scales, rotations, density_r, density_i))
+        dev = plan.device
+        if int(params[0].shape[0]) != plan.n:
+            raise ValueError(f"static plan is sized for {plan.n} Gaussians, got {int(params[0].shape[0])}")
+        st = _stream(dev)
+        gp = GsvParams(*(t.data_ptr() for t in params), plan.n)
+        check(lib.gsv_prepare(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), plan.gauss_bytes, None, st),
+              "gsv_prepare")
+        check(lib.gsv_bin(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.pair_bytes,
+                          plan.capacity, st), "gsv_bin")
+        vol = torch.empty((plan.shape.d, plan.shape.h, plan.shape.w), dtype=torch.complex64, device=dev)
+        check(lib.gsv_forward(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
+                              _ptr(vol), st), "gsv_forward")
+        ctx.plan = plan
+        ctx.save_for_backward(*params)
+        return vol
+
+    @staticmethod
+    def backward(ctx, grad_vol):
+        params = ctx.saved_tensors
+        g = grad_vol.resolve_conj().to(torch.complex64).contiguous()
+        outs = [torch.empty_like(t) for t in params]
+        backward_into(ctx.plan, params, g, outs)
+        return (*outs, None)
+
+
 def voxelize(positions: torch.Tensor, scales: torch.Tensor, rotations: torch.Tensor,
              density_r: torch.Tensor, density_i: torch.Tensor, volume_shape, tile_size: int = 8,
              deterministic: bool = False) -> torch.Tensor:
@@ -287,9 +337,44 @@ class TileVoxelizer(nn.Module):
             dr, di = density, torch.zeros_like(density)
         return _VoxelizeFn.apply(positions, scales, rotations, dr, di, self._shape, self.deterministic)
 
+    def static(self, n: int, capacity: int) -> "StaticVoxelizer":
+        """A sync-free, allocation-free variant for `n` Gaussians and at most
+        `capacity` (tile, Gaussian) pairs, for CUDA-graph capture."""
+        flags = _lib.GSV_BACKWARD_DETERMINISTIC if self.deterministic else 0
+        dev = torch.device(self.device) if not isinstance(self.device, torch.device) else self.device
+        return StaticVoxelizer(StaticPlan(self._shape, int(n), dev, int(capacity), flags))
+
+    def count_pairs(self, positions: torch.Tensor, scales: torch.Tensor) -> int:
+        """Pair total of the current parameters (one host sync)."""
+        params = (_f32(positions), _f32(scales), _f32(positions).new_zeros(positions.shape[0], 4),
+                  _f32(positions).new_zeros(positions.shape[0]), _f32(positions).new_zeros(positions.shape[0]))
+        params[2][:, 0] = 1.0
+        plan = BinPlan(self._shape, int(positions.shape[0]), positions.device)
+        gp = GsvParams(*(t.data_ptr() for t in params), plan.n)
+        st = _stream(positions.device)
+        check(lib.gsv_prepare(ctypes.byref(gp), self._shape, _ptr(plan.ws_gauss), plan.gauss_bytes, None, st),
+              "gsv_prepare")
+        total, fl = plan.read_status(st)
+        _raise_flags(fl, total)
+        return total
+
     def extra_repr(self) -> str:
         return (f"volume_shape={self.volume_shape}, tile_size={self.tile_size}, "
                 f"backend={self.backend}, deterministic={self.deterministic}")
+
+
+class StaticVoxelizer:
+    """Callable with TileVoxelizer's forward signature over a StaticPlan."""
+
+    def __init__(self, plan: StaticPlan):
+        self.plan = plan
+
+    def __call__(self, positions, scales, rotations, density, chunk_size: int = 4096):
+        if torch.is_complex(density):
+            dr, di = density.real, density.imag
+        else:
+            dr, di = density, torch.zeros_like(density)
+        return _VoxelizeStaticFn.apply(positions, scales, rotations, dr, di, self.plan)
 
 
 def num_tiles(volume_shape, tile_size: int) -> int:

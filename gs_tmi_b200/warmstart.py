@@ -1,0 +1,296 @@
+"""Learned warm start for the plain 3DGSMR fit.
+
+A small MLP maps the zero-filled image around a seed voxel (a 5^3 complex
+patch = 250 values, plus the sampling density of the acquisition and the
+seed's intensity-seeded scale; padded to 256) to the initial parameters of
+the Gaussian at that seed: centre offset (3), log-scale (3), quaternion (4)
+and complex density (2); padded to 16 outputs.
+
+Network 256 -> 256 (GELU) -> 256 (GELU) -> 16 with BF16 weights and FP32
+accumulation.  Every matrix product of inference and training -- X W^T with
+the bias + GELU epilogue, dY W with the GELU' epilogue, and the split-K
+weight gradients dZ^T X -- runs on the hand-written tcgen05 kernel
+(``gsv_mlp_gemm``); FP32 master weights take Adam steps and are rounded to
+BF16 for the next step.
+
+Training data come from plain fits the method itself produces on synthetic
+phantoms (``training_case``): the target is the volume the plain fit
+reconstructs.  A training step renders the MLP's Gaussians with this
+package's voxelizer and back-propagates the relative L2 distance to that
+volume through the voxelizer's backward kernels, the decoding and the MLP's
+tcgen05 backward (``render_step``).  The intensity-seeded initialisation of
+the reference (``synthetic.from_image_init``) stays as the fallback -- an
+untrained network reproduces it exactly -- and as the judge through the
+final NMSE against the fully sampled phantom.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from typing import List, Optional, Tuple
+
+import torch
+
+from . import sense, synthetic
+from ._lib import check, lib
+
+IN, HID, OUT = 256, 256, 16
+N_TARGET = 12
+PATCH = 5
+EPI_F32, EPI_BIAS_GELU, EPI_GELU_GRAD, EPI_ATOMIC_F32 = 0, 1, 2, 3
+
+
+def _p(t: Optional[torch.Tensor]):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def gemm(a, a_strides, b, b_strides, M, N, K, epi, out_f32=None, out_bf16=None, z=None, bias=None,
+         c_strides=None, splits=1, err=None):
+    """C = A B^T on the tcgen05 kernel (see include/gsv.h, gsv_mlp_gemm)."""
+    if err is None:
+        err = torch.zeros(1, dtype=torch.int32, device=a.device)
+    c_sm, c_sn = c_strides if c_strides else (N, 1)
+    check(lib.gsv_mlp_gemm(_p(a), a_strides[0], a_strides[1], _p(b), b_strides[0], b_strides[1], M, N, K, splits,
+                           _p(bias), _p(out_f32), _p(out_bf16), _p(z), c_sm, c_sn, epi, _p(err),
+                           ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)), "gsv_mlp_gemm")
+    return err
+
+
+# ---------------------------------------------------------------------------
+# features and decoding
+# ---------------------------------------------------------------------------
+
+def image_scale(zero_filled: torch.Tensor) -> float:
+    return float(torch.quantile(zero_filled.abs().reshape(-1)[::7].float(), 0.999).clamp_min(1e-6))
+
+
+def patch_features(zero_filled: torch.Tensor, voxels: torch.Tensor, sampling_density: float,
+                   scale: float, log_base_scale: torch.Tensor) -> torch.Tensor:
+    """[N, 256] BF16 features: the 5^3 complex patch around each seed voxel
+    (zero outside the volume), real then imaginary parts, divided by `scale`;
+    then the sampling density of the acquisition and the log of the seed's
+    intensity-seeded scale (voxels); then zeros."""
+    dev = zero_filled.device
+    r = PATCH // 2
+    pad = torch.nn.functional.pad(zero_filled.real.unsqueeze(0).unsqueeze(0), (r,) * 6).squeeze()
+    padi = torch.nn.functional.pad(zero_filled.imag.unsqueeze(0).unsqueeze(0), (r,) * 6).squeeze()
+    off = torch.arange(PATCH, device=dev)
+    od, oh, ow = torch.meshgrid(off, off, off, indexing="ij")
+    d = voxels[:, 0:1] + od.reshape(1, -1)
+    h = voxels[:, 1:2] + oh.reshape(1, -1)
+    w = voxels[:, 2:3] + ow.reshape(1, -1)
+    feats = torch.zeros(voxels.shape[0], IN, device=dev, dtype=torch.float32)
+    feats[:, :125] = pad[d, h, w] / scale
+    feats[:, 125:250] = padi[d, h, w] / scale
+    feats[:, 250] = sampling_density
+    feats[:, 251] = log_base_scale
+    return feats.bfloat16()
+
+
+def seed_voxels(init: synthetic.GaussianSet, shape) -> torch.Tensor:
+    """Voxel index of each seed position (from_image places seeds at voxel centres)."""
+    s = torch.tensor(shape, dtype=torch.float32, device=init.positions.device)
+    cv = (init.positions + 1.0) * 0.5 * s - 0.5
+    return torch.minimum(torch.clamp(torch.round(cv), min=0), s - 1).long()
+
+
+def decode(out: torch.Tensor, seed_vox: torch.Tensor, base: synthetic.GaussianSet, shape, scale: float):
+    """Network outputs -> (positions, scales, rotations, density_r, density_i),
+    differentiable.  Every output is a correction of the intensity-seeded
+    Gaussian (zero output = the plain init): offsets bounded to half a voxel,
+    log-scale corrections bounded to +-1, a quaternion correction of the
+    identity, a density correction in units of the image scale."""
+    s = torch.tensor(shape, dtype=torch.float32, device=out.device)
+    cv = seed_vox.float() + 0.5 * torch.tanh(out[:, 0:3])
+    pos = (cv + 0.5) / s * 2 - 1
+    scales = base.scales * torch.exp(torch.tanh(out[:, 3:6]))
+    q = out[:, 6:10] * 0.25
+    q = torch.cat([1.0 + q[:, :1], q[:, 1:]], 1)
+    q = q / q.norm(dim=-1, keepdim=True)
+    return pos, scales, q, base.density_r + out[:, 10] * scale, base.density_i + out[:, 11] * scale
+
+
+# ---------------------------------------------------------------------------
+# the network
+# ---------------------------------------------------------------------------
+
+class WarmStartMLP:
+    def __init__(self, device="cuda:0", seed: int = 0, lr: float = 1e-3):
+        self.device = torch.device(device)
+        g = torch.Generator().manual_seed(seed)
+
+        def lin(o, i):
+            return (torch.randn(o, i, generator=g) * math.sqrt(2.0 / i)).to(self.device)
+
+        self.w = [lin(HID, IN), lin(HID, HID), lin(OUT, HID) * 0.1]
+        self.b = [torch.zeros(HID, device=self.device), torch.zeros(HID, device=self.device),
+                  torch.zeros(OUT, device=self.device)]
+        for t in self.w + self.b:
+            t.requires_grad_(False)
+        self.params = [torch.nn.Parameter(t) for t in self.w + self.b]
+        self.opt = torch.optim.Adam(self.params, lr=lr)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._sync_bf16()
+
+    def _sync_bf16(self):
+        self.wb = [p.detach().bfloat16().contiguous() for p in self.params[:3]]
+
+    def forward(self, x: torch.Tensor):
+        """x: [B, 256] BF16 -> standardized outputs [B, 16] FP32 and the cache."""
+        B = x.shape[0]
+        dev = x.device
+        z1 = torch.empty(B, HID, device=dev)
+        y1 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
+        gemm(x, (IN, 1), self.wb[0], (IN, 1), B, HID, IN, EPI_BIAS_GELU, out_bf16=y1, z=z1,
+             bias=self.params[3].detach(), err=self.err)
+        z2 = torch.empty(B, HID, device=dev)
+        y2 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
+        gemm(y1, (HID, 1), self.wb[1], (HID, 1), B, HID, HID, EPI_BIAS_GELU, out_bf16=y2, z=z2,
+             bias=self.params[4].detach(), err=self.err)
+        out = torch.empty(B, OUT, device=dev)
+        gemm(y2, (HID, 1), self.wb[2], (HID, 1), B, OUT, HID, EPI_F32, out_f32=out, bias=self.params[5].detach(),
+             err=self.err)
+        return out, (x, z1, y1, z2, y2)
+
+    def backward(self, cache, dout: torch.Tensor) -> List[torch.Tensor]:
+        """Gradients of (W1, W2, W3, b1, b2, b3) for upstream dout [B, 16] FP32."""
+        x, z1, y1, z2, y2 = cache
+        B = x.shape[0]
+        dev = x.device
+        splits = max(1, min(64, B // 256))
+        dob = dout.bfloat16().contiguous()
+        dW3 = torch.zeros(OUT, HID, device=dev)
+        gemm(y2, (1, HID), dob, (1, OUT), HID, OUT, B, EPI_ATOMIC_F32, out_f32=dW3, c_strides=(1, HID),
+             splits=splits, err=self.err)
+        dz2 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
+        gemm(dob, (OUT, 1), self.wb[2], (1, HID), B, HID, OUT, EPI_GELU_GRAD, out_bf16=dz2, z=z2, err=self.err)
+        dW2 = torch.zeros(HID, HID, device=dev)
+        gemm(dz2, (1, HID), y1, (1, HID), HID, HID, B, EPI_ATOMIC_F32, out_f32=dW2, splits=splits, err=self.err)
+        dz1 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
+        gemm(dz2, (HID, 1), self.wb[1], (1, HID), B, HID, HID, EPI_GELU_GRAD, out_bf16=dz1, z=z1, err=self.err)
+        dW1 = torch.zeros(HID, IN, device=dev)
+        gemm(dz1, (1, HID), x, (1, IN), HID, IN, B, EPI_ATOMIC_F32, out_f32=dW1, splits=splits, err=self.err)
+        return [dW1, dW2, dW3, dz1.float().sum(0), dz2.float().sum(0), dout.sum(0)]
+
+    def check_ok(self):
+        if int(self.err.item()) != 0:
+            raise RuntimeError("tcgen05 GEMM wait timed out")
+
+    @torch.no_grad()
+    def predict(self, x: torch.Tensor) -> torch.Tensor:
+        out, _ = self.forward(x)
+        self.check_ok()
+        return out
+
+    def apply_grads(self, grads: List[torch.Tensor]):
+        for p, g in zip(self.params, grads):
+            p.grad = g
+        self.opt.step()
+        self._sync_bf16()
+
+    def state_dict(self):
+        return {"params": [p.detach().cpu() for p in self.params]}
+
+    def load_state_dict(self, sd):
+        for p, t in zip(self.params, sd["params"]):
+            p.data.copy_(t.to(self.device))
+        self._sync_bf16()
+
+
+# ---------------------------------------------------------------------------
+# training data from plain fits, training through the voxelizer, warm init
+# ---------------------------------------------------------------------------
+
+@dataclass
+class WarmConfig:
+    shape: Tuple[int, int, int] = (96, 96, 96)
+    n_coils: int = 8
+    accel: float = 6.0
+    calib: int = 24
+    points_per_voxel: float = 50_000 / (128 * 128 * 96)
+    fit_iterations: int = 1000
+
+
+@dataclass
+class TrainingCase:
+    shape: Tuple[int, int, int]
+    features: torch.Tensor        # [N, 256] BF16
+    seed_vox: torch.Tensor        # [N, 3]
+    base: synthetic.GaussianSet   # intensity-seeded Gaussians (the plain init)
+    scale: float
+    target: torch.Tensor          # complex64 volume of the plain fit
+
+
+def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device):
+    dev = torch.device(device)
+    base = synthetic.from_image_init(case.zero_filled, num_points, seed=seed).to(dev)
+    shape = tuple(case.ground_truth.shape)
+    zf = case.zero_filled.to(dev)
+    scale = image_scale(zf)
+    vox = seed_voxels(base, shape)
+    s = torch.tensor(shape, dtype=torch.float32, device=dev)
+    log_base = torch.log(base.scales[:, 0] * s.max() * 0.5)
+    x = patch_features(zf, vox, float(case.mask.mean()), scale, log_base)
+    return x, vox, base, scale
+
+
+def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
+    """A synthetic phantom, its intensity-seeded Gaussians and the volume the
+    plain method reconstructs from them (the training target)."""
+    case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed)
+    n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
+    x, vox, base, scale = case_inputs(case, n, seed + 1, device)
+    cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=10 ** 9)
+    res = sense.fit(case, base, cfg, device=device, eval_ssim=False)
+    from .tile_voxelizer import TileVoxelizer
+
+    vz = TileVoxelizer(wc.shape, device=device)
+    p = res.params
+    with torch.no_grad():
+        target = vz(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
+    return TrainingCase(wc.shape, x, vox, base, scale, target.detach())
+
+
+def render_step(mlp: WarmStartMLP, tc: TrainingCase, vox) -> float:
+    """One training step: MLP -> decode -> voxelize -> relative L2 to the
+    plain fit's volume; gradients back through the voxelizer's backward and
+    the MLP's tcgen05 backward."""
+    out, cache = mlp.forward(tc.features)
+    out = out.requires_grad_(True)
+    pos, scl, rot, dr, di = decode(out, tc.seed_vox, tc.base, tc.shape, tc.scale)
+    vol = vox(pos, scl, rot, torch.complex(dr, di))
+    diff = vol - tc.target
+    loss = (diff.real.square().sum() + diff.imag.square().sum()) / tc.target.abs().square().sum()
+    loss.backward()
+    mlp.apply_grads(mlp.backward(cache, out.grad))
+    return float(loss.detach())
+
+
+def train(mlp: WarmStartMLP, cases: List[TrainingCase], steps: int = 1500, seed: int = 0, log=None) -> List[float]:
+    from .tile_voxelizer import TileVoxelizer
+
+    voxes = {}
+    g = torch.Generator().manual_seed(seed)
+    losses = []
+    for i in range(steps):
+        tc = cases[int(torch.randint(0, len(cases), (1,), generator=g))]
+        if tc.shape not in voxes:
+            voxes[tc.shape] = TileVoxelizer(tc.shape, device=str(mlp.device))
+        losses.append(render_step(mlp, tc, voxes[tc.shape]))
+        if log and (i % 100 == 0 or i == steps - 1):
+            log({"step": i, "loss": losses[-1]})
+    mlp.check_ok()
+    return losses
+
+
+@torch.no_grad()
+def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed: int = 0,
+              device="cuda:0") -> synthetic.GaussianSet:
+    """Seeds exactly as the intensity-seeded init (same seed -> same voxels
+    and scales), parameters from the MLP."""
+    x, vox, base, scale = case_inputs(case, num_points, seed, device)
+    out = mlp.predict(x)
+    pos, scl, rot, dr, di = decode(out, vox, base, tuple(case.ground_truth.shape), scale)
+    return synthetic.GaussianSet(pos.contiguous(), scl.contiguous(), rot.contiguous(), dr.contiguous(),
+                                 di.contiguous())

@@ -131,6 +131,12 @@ GSV_API int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, 
 GSV_API int gsv_bin_views(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, int64_t capacity,
                   int32_t** tile_ranges, int32_t** pair_ids);
 
+/* Device addresses of the latched status flags (int32) and of the pair
+ * total (int64) inside ws_gauss, for asynchronous checks (e.g. a copy to
+ * pinned host memory captured in a CUDA graph). */
+GSV_API int gsv_status_views(gsv_shape shape, int64_t n, void* ws_gauss, int32_t** flags,
+                             int64_t** total_pairs);
+
 /* Read the pair total and latched flags (SYNCHRONISES the stream). */
 GSV_API int gsv_read_status(gsv_shape shape, int64_t n, const void* ws_gauss, int64_t* total_pairs,
                     int32_t* flags, void* stream);
@@ -178,6 +184,22 @@ GSV_API int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss
 GSV_API int gsv_build_tile_pairs_noalloc(const float* center_vox, const float* radius_vox, int64_t n,
                                          gsv_shape shape, int32_t* tile_ranges, int32_t* pair_ids,
                                          int64_t pair_capacity, int64_t* total_pairs, void* stream);
+
+/* ---- learned warm start: BF16 tensor-core GEMM (tcgen05, sm_100a) ----- */
+
+/* No counterpart in the reference (the warm-start MLP is an addition).
+ * C[m,n] = sum_k A[m,k] B[n,k] with BF16 operands read through element
+ * strides (A(m,k) = a[m*a_sm + k*a_sk], B(n,k) = b[n*b_sn + k*b_sk]) and FP32
+ * accumulation in tensor memory; C(m,n) lands at index m*c_sm + n*c_sn.
+ * epi: 0 = FP32 store of acc (+ bias[n] if bias), 1 = z_f32 = acc + bias,
+ * out_bf16 = GELU(z), 2 = out_bf16 = acc * GELU'(z_f32), 3 = atomicAdd of
+ * acc into out_f32 (required when splits > 1: K split across CTAs).
+ * N must be a multiple of 16.  *error (device int) becomes 1 if a wait on
+ * the tensor cores timed out. */
+GSV_API int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, long long b_sn,
+                         long long b_sk, int M, int N, int K, int splits, const float* bias, float* out_f32,
+                         void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, int* error,
+                         void* stream);
 
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 

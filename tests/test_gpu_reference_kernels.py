@@ -12,45 +12,14 @@ import torch
 
 import gs_tmi_b200
 from gs_tmi_b200 import synthetic
-from oracle import build_ref, torch_port
+from oracle import torch_port
 from tests.helpers import SMALL_CASES, load, rel
 
 pytestmark = pytest.mark.gpu
 
-REF = build_ref.load()
+from tests.helpers_ref import REF, reference_step  # noqa: E402
+
 needs_ref = pytest.mark.skipif(REF is None, reason="reference extension not built (oracle/build_ref.py)")
-
-
-class _RefFn(torch.autograd.Function):
-    """The reference's autograd glue (tile_voxelizer.py:165-207) over its compiled kernels."""
-
-    @staticmethod
-    def forward(ctx, center, cov_inv, dr, di, tr, pid, hs, ts, d, h, w):
-        vr, vi = REF.forward(center.contiguous(), cov_inv.contiguous(), dr.contiguous(), di.contiguous(), tr, pid,
-                             hs, ts, d, h, w)
-        ctx.save_for_backward(center, cov_inv, dr, di, tr, pid, hs)
-        ctx.dims = (ts, d, h, w)
-        return vr, vi
-
-    @staticmethod
-    def backward(ctx, gr, gi):
-        center, cov_inv, dr, di, tr, pid, hs = ctx.saved_tensors
-        ts, d, h, w = ctx.dims
-        gc, gm, gdr, gdi = REF.backward(center.contiguous(), cov_inv.contiguous(), dr.contiguous(), di.contiguous(),
-                                        tr, pid, hs, gr.contiguous(), gi.contiguous(), ts, d, h, w)
-        return gc, gm, gdr, gdi, None, None, None, None, None, None, None
-
-
-def reference_step(params, shape, ts):
-    """TileVoxelizer.forward of the reference on the GPU (tile_voxelizer.py:279-309):
-    torch preprocess, torch binning (host sync), its CUDA kernels."""
-    pos, scl, rot, dr, di = params
-    center, cov_inv, half = torch_port.preprocess(pos, scl, rot, shape)
-    with torch.no_grad():
-        tr, pid = torch_port.build_tile_pairs_torch(center.detach(), torch_port.radius_vox(scl.detach(), half),
-                                                    shape, ts)
-    vr, vi = _RefFn.apply(center, cov_inv, dr, di, tr, pid, half, ts, *shape)
-    return torch.complex(vr, vi).view(*shape)
 
 
 def _boundary_free(z):

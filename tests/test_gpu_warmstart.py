@@ -1,0 +1,164 @@
+"""Learned warm start: the MLP's tcgen05 forward/backward against a CPU
+reference, training, and what the trained network gains over the
+intensity-seeded initialisation.
+
+GSV_WARM_FULL=1 runs the full evaluation (training phantoms at 96^3, held-out
+128x128x96 R=6 phantoms, iterations and wall time to the plain method's final
+NMSE) and writes $GSV_REPORT_DIR/warmstart_eval.json."""
+import json
+import math
+import os
+import time
+
+import pytest
+import torch
+
+import gs_tmi_b200
+from gs_tmi_b200 import sense, synthetic, warmstart
+
+pytestmark = pytest.mark.gpu
+
+
+def _cpu_reference(mlp, x, dout):
+    """FP64 CPU forward/backward of the same network, with the BF16 roundings
+    the GPU path applies to operands (activations, upstream gradients)."""
+    bf = lambda t: t.to(torch.bfloat16).double()
+    W = [bf(w.detach().cpu()) for w in mlp.params[:3]]
+    b = [p.detach().cpu().double() for p in mlp.params[3:]]
+    xc = bf(x.cpu())
+    g = lambda z: 0.5 * z * (1 + torch.erf(z / math.sqrt(2)))
+    gp = lambda z: 0.5 * (1 + torch.erf(z / math.sqrt(2))) + z * torch.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    z1 = xc @ W[0].t() + b[0]
+    y1 = bf(g(z1))
+    z2 = y1 @ W[1].t() + b[1]
+    y2 = bf(g(z2))
+    out = y2 @ W[2].t() + b[2]
+    do = bf(dout.cpu())
+    dW3 = do.t() @ y2
+    dz2 = bf((do @ W[2]) * gp(z2))
+    dW2 = dz2.t() @ y1
+    dz1 = bf((dz2 @ W[1]) * gp(z1))
+    dW1 = dz1.t() @ xc
+    return out, [dW1, dW2, dW3, dz1.sum(0), dz2.sum(0), dout.cpu().double().sum(0)]
+
+
+def rel(a, b):
+    return float((a.double().cpu() - b).norm() / b.norm().clamp_min(1e-30))
+
+
+def test_mlp_forward_backward_vs_cpu(cuda_device):
+    mlp = warmstart.WarmStartMLP(str(cuda_device), seed=1)
+    g = torch.Generator(device=cuda_device).manual_seed(2)
+    B = 1536
+    x = torch.randn(B, 256, device=cuda_device, generator=g).bfloat16()
+    dout = torch.randn(B, 16, device=cuda_device, generator=g) / B
+    out, cache = mlp.forward(x)
+    grads = mlp.backward(cache, dout)
+    torch.cuda.synchronize()
+    mlp.check_ok()
+    ro, rg = _cpu_reference(mlp, x, dout)
+    assert rel(out, ro) < 5e-3
+    for name, a, b in zip(("dW1", "dW2", "dW3", "db1", "db2", "db3"), grads, rg):
+        assert rel(a, b) < 2e-2, name
+
+
+def test_mlp_regression_training(cuda_device):
+    """The MLP's own forward/backward kernels fit a smooth regression target."""
+    mlp = warmstart.WarmStartMLP(str(cuda_device), seed=3, lr=2e-3)
+    g = torch.Generator(device=cuda_device).manual_seed(4)
+    x = torch.randn(8192, 256, device=cuda_device, generator=g)
+    proj = torch.randn(256, 16, device=cuda_device, generator=g) / 16
+    t = torch.tanh(x @ proj)
+    xb = x.bfloat16()
+    losses = []
+    for i in range(300):
+        idx = torch.randint(0, 8192, (2048,), device=cuda_device, generator=g)
+        out, cache = mlp.forward(xb[idx])
+        diff = out - t[idx]
+        losses.append(float((diff * diff).mean()))
+        mlp.apply_grads(mlp.backward(cache, 2 * diff / diff.numel()))
+    mlp.check_ok()
+    assert sum(losses[-20:]) / 20 < 0.25 * sum(losses[:5]) / 5
+
+
+def _small_warm_setup(device):
+    wc = warmstart.WarmConfig(shape=(40, 40, 40), n_coils=4, accel=4.0, calib=12, fit_iterations=300)
+    cases = [warmstart.training_case(100 + 10 * s, wc, device=device) for s in range(6)]
+    mlp = warmstart.WarmStartMLP(device, seed=0)
+    losses = warmstart.train(mlp, cases, steps=1000)
+    return wc, mlp, losses
+
+
+def test_warm_start_gains_over_intensity_seeding(cuda_device):
+    """Held-out phantom: the trained network's Gaussians start closer to the
+    target than the intensity-seeded ones and stay ahead over the first
+    iterations of the same fit."""
+    dev = str(cuda_device)
+    wc, mlp, losses = _small_warm_setup(dev)
+    assert sum(losses[-20:]) / 20 < 0.8 * sum(losses[:5]) / 5
+    case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=999)
+    n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
+    plain_init = synthetic.from_image_init(case.zero_filled, n, seed=7)
+    warm = warmstart.warm_init(mlp, case, n, seed=7, device=dev)
+    gt = case.ground_truth.to(cuda_device)
+    vox = gs_tmi_b200.TileVoxelizer(wc.shape, device=dev)
+    raw = {}
+    for name, gs in (("plain", plain_init.to(cuda_device)), ("warm", warm)):
+        v = vox(gs.positions, gs.scales, gs.rotations, torch.complex(gs.density_r, gs.density_i))
+        raw[name] = sense.nmse(v, gt)
+    assert raw["warm"] < 0.85 * raw["plain"]
+    cfg = sense.FitConfig(iterations=101, eval_every=50, densify_from=10 ** 9)
+    p = sense.fit(case, plain_init, cfg, device=dev, eval_ssim=False)
+    w = sense.fit(case, warm, cfg, device=dev, eval_ssim=False)
+    assert w.history[0]["nmse"] < p.history[0]["nmse"]
+    assert w.history[-1]["nmse"] < p.history[-1]["nmse"]
+
+
+@pytest.mark.skipif(os.environ.get("GSV_WARM_FULL") != "1", reason="set GSV_WARM_FULL=1")
+def test_full_time_to_nmse(cuda_device):
+    dev = str(cuda_device)
+    wc = warmstart.WarmConfig()
+    n_train = int(os.environ.get("GSV_WARM_TRAIN_PHANTOMS", "48"))
+    n_eval = int(os.environ.get("GSV_WARM_EVAL_PHANTOMS", "4"))
+    t0 = time.perf_counter()
+    cases = [warmstart.training_case(1000 + 17 * s, wc, device=dev) for s in range(n_train)]
+    t_data = time.perf_counter() - t0
+    mlp = warmstart.WarmStartMLP(dev, seed=0)
+    t0 = time.perf_counter()
+    losses = warmstart.train(mlp, cases, steps=int(os.environ.get("GSV_WARM_STEPS", "2000")))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    shape = (128, 128, 96)
+    cfg = sense.FitConfig(iterations=2000, eval_every=25, max_points=500_000)
+    rows = []
+    for e in range(n_eval):
+        case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e)
+        plain = sense.fit(case, synthetic.from_image_init(case.zero_filled, 50_000, seed=e), cfg, device=dev,
+                          eval_ssim=True)
+        target = plain.final_nmse
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        warm = warmstart.warm_init(mlp, case, 50_000, seed=e, device=dev)
+        torch.cuda.synchronize()
+        t_init = time.perf_counter() - t0
+        w = sense.fit(case, warm, cfg, device=dev, stop_nmse=target, eval_ssim=True)
+        reached = [h for h in w.history if h["nmse"] <= target]
+        it = reached[0]["iteration"] if reached else None
+        secs = (reached[0]["seconds"] + t_init) if reached else None
+        rows.append({"phantom": e, "plain_final_nmse": target, "plain_final_ssim": plain.final_ssim,
+                     "plain_seconds": plain.seconds, "plain_nmse_at_0": plain.history[0]["nmse"],
+                     "warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": it,
+                     "warm_seconds_to_target": secs, "warm_init_seconds": t_init,
+                     "wall_ratio": (secs / plain.seconds) if secs else None})
+    report = {"train_phantoms": n_train, "train_examples": int(sum(c.features.shape[0] for c in cases)),
+              "data_seconds": t_data, "train_seconds": t_train, "final_train_loss": losses[-1],
+              "eval": rows}
+    ratios = [r["wall_ratio"] for r in rows if r["wall_ratio"] is not None]
+    report["median_wall_ratio"] = sorted(ratios)[len(ratios) // 2] if ratios else None
+    out = os.environ.get("GSV_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "warmstart_eval.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    print(json.dumps({k: v for k, v in report.items() if k != "eval"}), json.dumps(rows))
+    assert all(r["warm_nmse_at_0"] < r["plain_nmse_at_0"] for r in rows)

@@ -1,0 +1,83 @@
+"""Host logic of the SENSE loop on the CPU: the loop, density control and
+Adam-state transplant run with the CPU port of the reference voxelizer
+(oracle/torch_port.py) standing in for the CUDA library."""
+import numpy as np
+import torch
+
+from gs_tmi_b200 import sense, synthetic
+from oracle import torch_port
+
+
+def cpu_voxelizer(shape, ts=4):
+    def vox(positions, scales, rotations, density):
+        center, cov_inv, half = torch_port.preprocess(positions, scales, rotations, shape)
+        with torch.no_grad():
+            tr, pid = torch_port.build_tile_pairs_torch(center.detach(), torch_port.radius_vox(scales.detach(), half),
+                                                        shape, ts)
+        tiles = range(tr.shape[0])
+        return torch_port.tile_forward(center, cov_inv, density, half, tr.numpy(), pid.numpy(), shape, ts,
+                                       tiles).view(*shape)
+    return vox
+
+
+def test_fit_loop_and_density_control_on_cpu():
+    shape = (16, 16, 12)
+    case = synthetic.mri_case(shape, n_coils=2, accel=3.0, calib=6, seed=3)
+    init = synthetic.from_image_init(case.zero_filled, 300, seed=4)
+    cfg = sense.FitConfig(iterations=25, densify_from=5, densify_every=10, densify_until=25, eval_every=8,
+                          grad_threshold=1e-4, scale_threshold=0.05, max_points=2000)
+    rows = []
+    res = sense.fit(case, init, cfg, voxelizer=cpu_voxelizer(shape), device="cpu", log=rows.append,
+                    eval_ssim=True)
+    assert len(rows) >= 3
+    assert min(r["loss"] for r in rows[1:]) < rows[0]["loss"]
+    assert all(np.isfinite(r["nmse"]) for r in rows)
+    ns = [r["n_points"] for r in rows]
+    assert max(ns) != 300 or min(ns) != 300  # density control fired
+    p = res.params
+    assert all(t.shape[0] == p.n for t in p.tensors())
+    assert np.isfinite(res.final_nmse) and 0 < res.final_ssim <= 1
+
+
+def test_transplant_keeps_moments_of_surviving_rows():
+    shape = (8, 8, 8)
+    gs = synthetic.random_gaussians(10, shape, seed=1)
+    p = sense.GaussianParams(gs, "cpu")
+    cfg = sense.FitConfig()
+    opt = sense.make_optimizer(p, cfg, fused=False)
+    for t in p.tensors():
+        t.grad = torch.randn_like(t)
+    opt.step()
+    keep = torch.tensor([True, False] * 5)
+    old = [opt.state[t]["exp_avg"].clone() for t in p.tensors()]
+    p.replace([torch.cat([t[keep], t[:3]]) for t in p.tensors()])
+    new_opt = sense.make_optimizer(p, cfg, fused=False)
+    sense.transplant(opt, new_opt, keep, p.n)
+    for o, t in zip(old, p.tensors()):
+        st = new_opt.state[t]["exp_avg"]
+        assert st.shape[0] == 8
+        assert torch.equal(st[:5], o[keep]) and not st[5:].any()
+
+
+def test_metrics():
+    g = torch.Generator().manual_seed(0)
+    x = torch.complex(torch.rand(12, 12, 12, generator=g), torch.rand(12, 12, 12, generator=g))
+    assert sense.nmse(x, x) == 0.0
+    assert abs(sense.ssim3d(x, x) - 1.0) < 1e-12
+    y = x + 0.05 * torch.rand(12, 12, 12, generator=g)
+    assert 0 < sense.ssim3d(y, x) < 1 and sense.nmse(y, x) > 0
+    # SSIM against a direct evaluation of the definition at one window
+    a, b = x.abs().double().numpy(), y.abs().double().numpy()
+    L = b.max() - b.min()
+    wa, wb = a[:7, :7, :7].ravel(), b[:7, :7, :7].ravel()
+    c1, c2 = (0.01 * L) ** 2, (0.03 * L) ** 2
+    s = ((2 * wa.mean() * wb.mean() + c1) * (2 * np.cov(wa, wb)[0, 1] + c2)) / (
+        (wa.mean() ** 2 + wb.mean() ** 2 + c1) * (wa.var(ddof=1) + wb.var(ddof=1) + c2))
+    import torch.nn.functional as F  # noqa: F401
+
+    xa = torch.tensor(a)[None, None]
+    yb = torch.tensor(b)[None, None]
+    one = sense.ssim3d(torch.tensor(a[:7, :7, :7]).to(torch.complex128), torch.tensor(b[:7, :7, :7]).to(torch.complex128),
+                       data_range=L)
+    assert abs(one - s) < 1e-10
+    del xa, yb
