@@ -35,8 +35,14 @@ import torch
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+BATCH12 = [((96, 96, 96), 30_000), ((112, 112, 96), 100_000), ((128, 128, 96), 170_000),
+           ((128, 128, 128), 240_000), ((144, 144, 112), 310_000), ((160, 160, 96), 380_000),
+           ((160, 160, 128), 450_000), ((176, 176, 112), 520_000), ((192, 192, 128), 590_000),
+           ((208, 208, 112), 660_000), ((224, 224, 96), 730_000), ((224, 224, 128), 800_000)]
+
 WORKLOADS = {
     "mri128x128x96_n50k": dict(shape=(128, 128, 96), n=50_000, kind="from_image"),
+    "batch12": dict(shape=None, n=sum(n for _, n in BATCH12), kind="batch"),
     "mri128x128x96_n500k": dict(shape=(128, 128, 96), n=500_000, kind="from_image"),
     "cube64_n20k": dict(shape=(64, 64, 64), n=20_000, kind="random"),
 }
@@ -57,6 +63,120 @@ def make_inputs(name):
     else:
         gs = synthetic.random_gaussians(wl["n"], wl["shape"], seed=0)
     return gs, synthetic.upstream_grad(wl["shape"], seed=1)
+
+
+def make_batch_inputs():
+    """Twelve phantoms of uneven size, each with intensity-seeded Gaussians
+    (30k..800k) and a complex standard-normal upstream gradient."""
+    from gs_tmi_b200 import synthetic
+
+    out = []
+    for i, (shape, n) in enumerate(BATCH12):
+        img = synthetic.ellipsoid_phantom(shape, seed=100 + i)
+        gs = synthetic.from_image_init(img, n, seed=100 + i)
+        out.append((shape, gs, synthetic.upstream_grad(shape, seed=200 + i)))
+    return out
+
+
+def run_batched(args, rank, world, dist):
+    """One iteration = binning of all twelve volumes + ONE persistent forward
+    launch + ONE persistent backward launch, captured as one CUDA graph."""
+    from gs_tmi_b200 import batched
+    from gs_tmi_b200.tile_voxelizer import TileVoxelizer
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    items = make_batch_inputs()
+    caps, evals = [], 0
+    for shape, gs, _ in items:
+        vz = TileVoxelizer(shape, device=str(dev))
+        total = vz.count_pairs(gs.positions.to(dev), gs.scales.to(dev))
+        caps.append(int(total * 1.1) + 1024)
+        plan = __import__("gs_tmi_b200").prepare_and_bin(tuple(t.to(dev) for t in gs.tensors()),
+                                                         vz._shape)
+        tr_ptr, _ = plan.views()
+        nt = lib_num_tiles(vz._shape)
+        off = tr_ptr - plan.ws_gauss.data_ptr()
+        tr = plan.ws_gauss[off:off + 8 * nt].view(torch.int32).reshape(-1, 2).cpu().numpy()
+        evals += evals_of(tr, shape)
+    sb = batched.StaticBatch([s for s, _, _ in items], [gs.n for _, gs, _ in items], caps, device=str(dev),
+                             deterministic=args.deterministic)
+    for i, (shape, gs, gv) in enumerate(items):
+        for dst, src in zip(sb.params[i], gs.tensors()):
+            dst.copy_(src.to(dev))
+        sb.grad_volumes[i].copy_(gv.to(dev))
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            sb.bin()
+            sb.forward()
+            sb.backward()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    torch.cuda.synchronize(dev)
+    if any(sb.overflowed()):
+        raise RuntimeError("pair capacity overflow in the batched benchmark")
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        sb.bin()
+        sb.forward()
+        sb.backward()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    cur = torch.cuda.current_stream(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(cur)
+            graph.replay()
+            ev[i][1].record(cur)
+        torch.cuda.synchronize(dev)
+    lat = sorted(a.elapsed_time(b) for a, b in ev)
+    total_ms = sum(lat)
+    stats = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
+    total_ms = float(stats[0])
+    if rank != 0:
+        return
+    out = {"metric": "fwd+bwd Gvox-evals/s", "value": evals * args.steps * world / (total_ms * 1e-3) / 1e9,
+           "unit": "Gvox-evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32", "data": "synthetic",
+           "config": {"workload": "batch12", "volumes": [list(s) for s, _ in BATCH12],
+                      "gaussians": [n for _, n in BATCH12], "tile_size": TILE, "evals_per_step": evals,
+                      "launch": "per-volume binning + 1 persistent forward + 1 persistent backward (+zero, "
+                                "finalize), one CUDA graph per iteration",
+                      "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
+           "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                          "min": lat[0], "max": lat[-1]},
+           "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
+
+
+def lib_num_tiles(gshape):
+    from gs_tmi_b200._lib import lib
+
+    return int(lib.gsv_num_tiles(gshape))
+
+
+def evals_of(tr, shape):
+    d, h, w = shape
+    nth, ntw = -(-h // TILE), -(-w // TILE)
+    e = 0
+    for t in range(tr.shape[0]):
+        td, rem = divmod(t, nth * ntw)
+        th, tw = divmod(rem, ntw)
+        nv = min(TILE, d - td * TILE) * min(TILE, h - th * TILE) * min(TILE, w - tw * TILE)
+        e += int(tr[t, 1] - tr[t, 0]) * nv
+    return e
 
 
 def peaks():
@@ -381,7 +501,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, dist)
+        if args.workload == "batch12":
+            run_batched(args, rank, world, dist)
+        else:
+            run_ours(args, rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -42,6 +42,12 @@ class GsvGrads(ctypes.Structure):
                 ("density_i", ctypes.c_void_p)]
 
 
+class GsvBatchItem(ctypes.Structure):
+    _fields_ = [("shape", GsvShape), ("params", GsvParams), ("ws_gauss", ctypes.c_void_p),
+                ("ws_pairs", ctypes.c_void_p), ("capacity", ctypes.c_int64), ("volume", ctypes.c_void_p),
+                ("grad_volume", ctypes.c_void_p), ("grads", GsvGrads)]
+
+
 # name -> (restype, argtypes); the complete exported C ABI.
 _vp, _i32, _i64, _sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -61,6 +67,10 @@ SIGNATURES = {
     "gsv_read_status": (ctypes.c_int, [_S, _i64, _vp, _i64p, _i32p, _vp]),
     "gsv_forward": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, _vp, _vp]),
     "gsv_backward": (ctypes.c_int, [_P, _S, _vp, _vp, _i64, _vp, _G, ctypes.c_int, _vp]),
+    "gsv_batch_workspace_bytes": (_sz, [ctypes.c_int]),
+    "gsv_batch_setup": (ctypes.c_int, [ctypes.POINTER(GsvBatchItem), ctypes.c_int, ctypes.c_int, _vp, _sz, _vp]),
+    "gsv_forward_batched": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "gsv_backward_batched": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
     "gsv_build_tile_pairs_count": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _sz, _i64p, _vp]),
     "gsv_build_tile_pairs_fill": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp, _vp, _vp]),
     "gsv_build_tile_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _vp, _i64, _i64p, _vp]),

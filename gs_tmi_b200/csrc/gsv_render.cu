@@ -65,6 +65,10 @@ struct RenderArgs {
     float* g_cov;
     float* g_dr;
     float* g_di;
+    // finalize
+    gsv_params prm;
+    gsv_grads grd;
+    const int4* boxes;
 };
 
 template <bool COMPAT>
@@ -195,13 +199,14 @@ struct __align__(16) WarpStage {
     int32_t gid[32];
 };
 
-template <bool COMPAT, bool PLANAR>
-__global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
-    __shared__ __align__(16) unsigned char smem_raw[kWarps * 16 * 32 * sizeof(float2)];
-    WarpStage* stage = reinterpret_cast<WarpStage*>(smem_raw);
-    static_assert(sizeof(WarpStage) * kWarps <= sizeof(smem_raw), "stage too large");
+constexpr int kFwdSmem = kWarps * 16 * 32 * sizeof(float2);
+static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 
-    const int64_t tile = blockIdx.x;
+// One 8^3 tile of the forward.  Contains two CTA barriers; every thread of
+// the CTA must call it for the same tile.
+template <bool COMPAT, bool PLANAR>
+__device__ __forceinline__ void forward_tile8(const RenderArgs& a, int64_t tile, unsigned char* smem_raw) {
+    WarpStage* stage = reinterpret_cast<WarpStage*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int d0, h0, w0;
     decode_tile(a, tile, d0, h0, w0);
@@ -241,16 +246,28 @@ __global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
                 const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
                 const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
                 float m[16];
-                bool any = false;
+                bool anyA = false, anyB = false;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     m[k] = row_m(g.q22, Aa, Ba, e2[k]);
                     m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
-                    any |= (m[k] <= kCut) | (m[8 + k] <= kCut);
+                    anyA |= (m[k] <= kCut);
+                    anyB |= (m[8 + k] <= kCut);
                 }
-                if (__any_sync(kFull, any)) {
+                // the exp / FMA part of each half-tile runs only if some lane needs it
+                if (__any_sync(kFull, anyA)) {
 #pragma unroll
-                    for (int k = 0; k < 16; ++k) {
+                    for (int k = 0; k < 8; ++k) {
+                        if (m[k] <= kCut) {
+                            const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
+                            accR[k] = fmaf(wgt, g.rho_r, accR[k]);
+                            accI[k] = fmaf(wgt, g.rho_i, accI[k]);
+                        }
+                    }
+                }
+                if (__any_sync(kFull, anyB)) {
+#pragma unroll
+                    for (int k = 8; k < 16; ++k) {
                         if (m[k] <= kCut) {
                             const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
                             accR[k] = fmaf(wgt, g.rho_r, accR[k]);
@@ -312,15 +329,19 @@ __global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
     }
 }
 
+template <bool COMPAT, bool PLANAR>
+__global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
+    __shared__ __align__(16) unsigned char smem_raw[kFwdSmem];
+    forward_tile8<COMPAT, PLANAR>(a, blockIdx.x, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // Tile edge 8: backward
 // ---------------------------------------------------------------------------
 
+// One 8^3 tile of the backward (warp-synchronous only, no CTA barrier).
 template <bool COMPAT, bool DET>
-__global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
-    __shared__ __align__(16) WarpStage stage[kWarps];
-
-    const int64_t tile = blockIdx.x;
+__device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile, WarpStage* stage) {
     const int2 rg = a.ranges[tile];
     if (rg.x >= rg.y) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -382,19 +403,22 @@ __global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
             const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
             const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
             float m[16];
-            bool any = false;
+            bool anyA = false, anyB = false;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 m[k] = row_m(g.q22, Aa, Ba, e2[k]);
                 m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
-                any |= (m[k] <= kCut) | (m[8 + k] <= kCut);
+                anyA |= (m[k] <= kCut);
+                anyB |= (m[8 + k] <= kCut);
             }
-            if (!__any_sync(kFull, any)) continue;
+            const bool wA = __any_sync(kFull, anyA), wB = __any_sync(kFull, anyB);
+            if (!(wA || wB)) continue;
             const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
             float R0[2] = {0.f, 0.f}, R1[2] = {0.f, 0.f}, R2[2] = {0.f, 0.f};
             float Dr = 0.f, Di = 0.f;
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
+                if (!(r == 0 ? wA : wB)) continue;  // warp-uniform half-tile skip
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int q = r * 8 + k;
@@ -439,6 +463,12 @@ __global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
         }
         __syncwarp();
     }
+}
+
+template <bool COMPAT, bool DET>
+__global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
+    __shared__ __align__(16) WarpStage stage[kWarps];
+    backward_tile8<COMPAT, DET>(a, blockIdx.x, stage);
 }
 
 // ---------------------------------------------------------------------------
@@ -582,11 +612,10 @@ __global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs 
 // ---------------------------------------------------------------------------
 
 template <bool DET>
-__global__ void __launch_bounds__(256) k_finalize(const gsv_params p, const RenderArgs a,
-                                                  const int4* __restrict__ boxes,
-                                                  gsv_grads out) {
-    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= p.n) return;
+__device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
+    const gsv_params& p = a.prm;
+    const gsv_grads& out = a.grd;
+    const int4* __restrict__ boxes = a.boxes;
     float mo[kMom];
     if (!DET) {
 #pragma unroll
@@ -686,6 +715,95 @@ __global__ void __launch_bounds__(256) k_finalize(const gsv_params p, const Rend
     for (int k = 0; k < 4; ++k) out.rotations[g * 4 + k] = gn[k] / den - q[k] * corr;
 }
 
+template <bool DET>
+__global__ void __launch_bounds__(256) k_finalize(const RenderArgs a) {
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= a.prm.n) return;
+    finalize_one<DET>(a, g);
+}
+
+// ---------------------------------------------------------------------------
+// Batched persistent launches: many volumes, one launch.  The descriptor
+// table (one RenderArgs per volume) and prefix sums of tiles, Gaussians and
+// pair capacities live in device memory; CTAs pull global tile indices from
+// an atomic counter until the work runs out.
+// ---------------------------------------------------------------------------
+
+struct BatchTable {
+    RenderArgs* items;
+    int64_t* tile_prefix;   // [count + 1]
+    int64_t* gauss_prefix;  // [count + 1]
+    int64_t* cap_prefix;    // [count + 1]
+    unsigned long long* counters;  // [2]: forward, backward work counters
+    int count;
+    int det;
+};
+
+__device__ __forceinline__ int find_item(const int64_t* prefix, int count, int64_t x) {
+    int lo = 0, hi = count;  // largest i with prefix[i] <= x
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kThreads) k_forward8_batched(const BatchTable t) {
+    __shared__ __align__(16) unsigned char smem_raw[kFwdSmem];
+    __shared__ long long s_next;
+    const int64_t total = t.tile_prefix[t.count];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = (long long)atomicAdd(&t.counters[0], 1ull);
+        __syncthreads();
+        const int64_t gt = s_next;
+        if (gt >= total) break;
+        const int i = find_item(t.tile_prefix, t.count, gt);
+        forward_tile8<false, false>(t.items[i], gt - t.tile_prefix[i], smem_raw);
+    }
+}
+
+template <bool DET>
+__global__ void __launch_bounds__(kThreads) k_backward8_batched(const BatchTable t) {
+    __shared__ __align__(16) WarpStage stage[kWarps];
+    __shared__ long long s_next;
+    const int64_t total = t.tile_prefix[t.count];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_next = (long long)atomicAdd(&t.counters[1], 1ull);
+        __syncthreads();
+        const int64_t gt = s_next;
+        if (gt >= total) break;
+        const int i = find_item(t.tile_prefix, t.count, gt);
+        backward_tile8<false, DET>(t.items[i], gt - t.tile_prefix[i], stage);
+    }
+}
+
+// Zero the gradient accumulators (or deterministic partials) of every volume.
+__global__ void k_zero_batched(const BatchTable t) {
+    const int64_t total = t.det ? t.cap_prefix[t.count] * kMomStride : t.gauss_prefix[t.count] * kMomStride;
+    const int64_t* prefix = t.det ? t.cap_prefix : t.gauss_prefix;
+    for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
+         x += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t row = x / kMomStride;
+        const int i = find_item(prefix, t.count, row);
+        const int64_t local = x - prefix[i] * kMomStride;
+        float* dst = t.det ? t.items[i].partials : t.items[i].accum;
+        dst[local] = 0.0f;
+    }
+}
+
+template <bool DET>
+__global__ void __launch_bounds__(256) k_finalize_batched(const BatchTable t) {
+    const int64_t total = t.gauss_prefix[t.count];
+    for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
+         x += int64_t(gridDim.x) * blockDim.x) {
+        const int i = find_item(t.gauss_prefix, t.count, x);
+        finalize_one<DET>(t.items[i], x - t.gauss_prefix[i]);
+    }
+}
+
 int grid_for(int64_t items, int block) {
     int64_t g = (items + block - 1) / block;
     return int(g < 1 ? 1 : g);
@@ -782,8 +900,11 @@ int gsv_backward(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* ws_
         }
         GSV_LAUNCH_CHECK();
     }
-    if (det) k_finalize<true><<<grid_for(n, 256), 256, 0, st>>>(*p, a, cat<int4>(ws_gauss, G.box), *grads);
-    else k_finalize<false><<<grid_for(n, 256), 256, 0, st>>>(*p, a, cat<int4>(ws_gauss, G.box), *grads);
+    a.prm = *p;
+    a.grd = *grads;
+    a.boxes = cat<int4>(ws_gauss, G.box);
+    if (det) k_finalize<true><<<grid_for(n, 256), 256, 0, st>>>(a);
+    else k_finalize<false><<<grid_for(n, 256), 256, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }
@@ -852,6 +973,121 @@ int gsv_tile_backward(const float* centers, const float* cov_inv, const float* d
     a.g_di = grad_den_i;
     if (tile_size == 8) k_backward8<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     else k_backward_generic<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+size_t gsv_batch_workspace_bytes(int count) {
+    if (count <= 0 || count > (1 << 16)) return 0;
+    return align_up(size_t(count) * sizeof(RenderArgs)) + 3 * align_up(size_t(count + 1) * sizeof(int64_t)) +
+           align_up(2 * sizeof(unsigned long long));
+}
+
+int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, void* ws_batch, size_t ws_bytes,
+                    void* stream) {
+    if (!items || count <= 0 || !ws_batch || ws_bytes < gsv_batch_workspace_bytes(count))
+        return GSV_ERR_INVALID_ARGUMENT;
+    const bool det = flags & GSV_BACKWARD_DETERMINISTIC;
+    RenderArgs* host = new RenderArgs[count];
+    int64_t* pre = new int64_t[3 * (count + 1)];
+    int64_t *tp = pre, *gp = pre + count + 1, *cp = pre + 2 * (count + 1);
+    tp[0] = gp[0] = cp[0] = 0;
+    int rc = GSV_OK;
+    for (int i = 0; i < count && rc == GSV_OK; ++i) {
+        const gsv_batch_item& it = items[i];
+        GaussLayout G;
+        PairLayout P;
+        int64_t ntiles = 0;
+        if (it.shape.tile_size != 8 || layout_for(it.shape, it.params.n, it.capacity, flags, &G, &P, &ntiles) != GSV_OK ||
+            !it.ws_gauss || (it.capacity > 0 && !it.ws_pairs)) {
+            rc = GSV_ERR_INVALID_ARGUMENT;
+            break;
+        }
+        RenderArgs a{};
+        fill_shape(a, it.shape);
+        a.recs = cat<Rec>(it.ws_gauss, G.rec);
+        a.ranges = cat<int2>(it.ws_gauss, G.ranges);
+        a.pair_ids = it.capacity > 0 ? cat<int32_t>(it.ws_pairs, P.vals_out) : nullptr;
+        a.vol = it.volume;
+        a.gvol = it.grad_volume;
+        a.accum = mat<float>(const_cast<void*>(it.ws_gauss), G.accum);
+        a.partials = det && it.capacity > 0 ? mat<float>(const_cast<void*>(it.ws_pairs), P.partials) : nullptr;
+        a.prm = it.params;
+        a.grd = it.grads;
+        a.boxes = cat<int4>(it.ws_gauss, G.box);
+        host[i] = a;
+        tp[i + 1] = tp[i] + ntiles;
+        gp[i + 1] = gp[i] + it.params.n;
+        cp[i + 1] = cp[i] + (det ? it.capacity : 0);
+    }
+    if (rc == GSV_OK) {
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        char* base = static_cast<char*>(ws_batch);
+        const size_t o_items = 0, o_pre = align_up(size_t(count) * sizeof(RenderArgs));
+        cudaError_t e = cudaMemcpyAsync(base + o_items, host, size_t(count) * sizeof(RenderArgs),
+                                        cudaMemcpyHostToDevice, st);
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+            e = cudaMemcpyAsync(base + o_pre + k * align_up(size_t(count + 1) * sizeof(int64_t)),
+                                pre + k * (count + 1), size_t(count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            gsv_detail_set_error(e, "gsv_batch_setup upload", __FILE__, __LINE__);
+            rc = GSV_ERR_CUDA;
+        }
+    }
+    delete[] host;
+    delete[] pre;
+    return rc;
+}
+
+namespace {
+BatchTable batch_table(void* ws_batch, int count, int det) {
+    BatchTable t{};
+    char* base = static_cast<char*>(ws_batch);
+    const size_t o_pre = align_up(size_t(count) * sizeof(RenderArgs));
+    const size_t step = align_up(size_t(count + 1) * sizeof(int64_t));
+    t.items = reinterpret_cast<RenderArgs*>(base);
+    t.tile_prefix = reinterpret_cast<int64_t*>(base + o_pre);
+    t.gauss_prefix = reinterpret_cast<int64_t*>(base + o_pre + step);
+    t.cap_prefix = reinterpret_cast<int64_t*>(base + o_pre + 2 * step);
+    t.counters = reinterpret_cast<unsigned long long*>(base + o_pre + 3 * step);
+    t.count = count;
+    t.det = det;
+    return t;
+}
+
+int persistent_grid() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 4;
+}
+}  // namespace
+
+int gsv_forward_batched(void* ws_batch, int count, void* stream) {
+    if (!ws_batch || count <= 0) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BatchTable t = batch_table(ws_batch, count, 0);
+    GSV_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 2 * sizeof(unsigned long long), st));
+    k_forward8_batched<<<persistent_grid(), kThreads, 0, st>>>(t);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream) {
+    if (!ws_batch || count <= 0) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool det = flags & GSV_BACKWARD_DETERMINISTIC;
+    BatchTable t = batch_table(ws_batch, count, det);
+    GSV_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 2 * sizeof(unsigned long long), st));
+    const int grid = persistent_grid();
+    k_zero_batched<<<grid, 256, 0, st>>>(t);
+    GSV_LAUNCH_CHECK();
+    if (det) k_backward8_batched<true><<<grid, kThreads, 0, st>>>(t);
+    else k_backward8_batched<false><<<grid, kThreads, 0, st>>>(t);
+    GSV_LAUNCH_CHECK();
+    if (det) k_finalize_batched<true><<<grid, 256, 0, st>>>(t);
+    else k_finalize_batched<false><<<grid, 256, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }

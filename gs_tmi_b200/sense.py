@@ -59,6 +59,7 @@ class FitConfig:
     deterministic: bool = False
     eval_every: int = 100
     seed: int = 0
+    capturable_adam: bool = False  # device-side LR/bias correction (what fit_graph uses)
 
 
 # ---------------------------------------------------------------------------
@@ -268,8 +269,10 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
     ku = case.kspace_undersampled.to(dev)
     gt = case.ground_truth.to(dev)
     p = GaussianParams(init, dev)
-    opt = make_optimizer(p, cfg)
     lrs = [cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr, cfg.density_lr]
+    if cfg.capturable_adam:
+        lrs = [torch.tensor(v, device=dev) for v in lrs]
+    opt = make_optimizer(p, cfg, lrs, capturable=cfg.capturable_adam)
     gen = torch.Generator(device=dev).manual_seed(cfg.seed)
     res = FitResult(params=p)
     mask_c = mask.unsqueeze(0)
@@ -296,7 +299,7 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
             lrs = [g["lr"] for g in opt.param_groups]
 
             def rebuild(keep, holder=holder, lrs=lrs):
-                new_opt = make_optimizer(p, cfg, lrs)
+                new_opt = make_optimizer(p, cfg, lrs, capturable=cfg.capturable_adam)
                 transplant(holder[0], new_opt, keep, p.n)
                 holder[0] = new_opt
 
@@ -305,6 +308,8 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
                 skip_sched = True
         if skip_sched:
             skip_sched = False
+        elif cfg.capturable_adam:
+            torch._foreach_mul_([g["lr"] for g in opt.param_groups], cfg.gamma)
         else:
             for g in opt.param_groups:
                 g["lr"] *= cfg.gamma
@@ -362,10 +367,14 @@ class _GraphedStep:
         for t in p.tensors():
             st = opt.state.get(t, {})
             self.state_tensors += [st[k] for k in ("exp_avg", "exp_avg_sq", "step") if k in st]
+        # Adam creates its state lazily at the first step: an undo before that
+        # must drop the state again
+        self.had_state = bool(self.state_tensors)
         self.live = p.tensors() + self.state_tensors
         self.snap = [torch.empty_like(t) for t in self.live]
         self.S, self.mask_c, self.ku = S, mask_c, ku
         self.graph = None
+        self.stream = torch.cuda.Stream(dev)
 
     def _body(self):
         torch._foreach_copy_(self.snap, self.live)
@@ -386,18 +395,33 @@ class _GraphedStep:
         self.flags_host.copy_(self.svox.plan.flags_dev, non_blocking=True)
 
     def eager(self):
-        """Run one real iteration outside the graph (also the capture warm-up)."""
+        """Run one real iteration outside the graph (also the capture warm-up),
+        on the stream the capture will use."""
         dev = self.p.positions.device
-        side = torch.cuda.Stream(dev)
-        side.wait_stream(torch.cuda.current_stream(dev))
-        with torch.cuda.stream(side):
+        self.stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(self.stream):
             self._body()
-        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.current_stream(dev).wait_stream(self.stream)
 
-    def capture(self):
+    def capture(self, pool=None):
+        """Capture the iteration.  capture_begin/end directly: torch.cuda.graph()
+        would empty the device and pinned-host allocator caches on every
+        (re)capture.  `pool` = the previous graph's memory pool: most large
+        buffers (volumes, k-space) do not depend on the Gaussian count and
+        are reused; the previous graph is never replayed again."""
+        dev = self.p.positions.device
         self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self._body()
+        self.stream.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(self.stream):
+            if pool is None:
+                self.graph.capture_begin()
+            else:
+                self.graph.capture_begin(pool=pool)
+            try:
+                self._body()
+            finally:
+                self.graph.capture_end()
+        torch.cuda.current_stream(dev).wait_stream(self.stream)
 
     def replay(self):
         self.graph.replay()
@@ -406,8 +430,12 @@ class _GraphedStep:
         torch.cuda.current_stream(self.p.positions.device).synchronize()
         return bool(int(self.flags_host[0]) & 1)
 
+    @torch.no_grad()
     def undo(self):
         torch._foreach_copy_(self.live, self.snap)
+        if not self.had_state:
+            for t in self.p.tensors():
+                self.opt.state.pop(t, None)
 
 
 def fit_graph(case: MRICase, init: GaussianSet, cfg: FitConfig, device="cuda:0", stop_nmse: Optional[float] = None,
@@ -437,18 +465,21 @@ def fit_graph(case: MRICase, init: GaussianSet, cfg: FitConfig, device="cuda:0",
     st = stats if stats is not None else {}
     st.setdefault("captures", 0)
     st.setdefault("overflows", 0)
+    st.setdefault("capture_seconds", 0.0)
 
     def new_step():
         cap = int(vox.count_pairs(p.positions.detach(), torch.exp(p.log_scales.detach())) * capacity_margin) + 4096
         return _GraphedStep(p, opt, vox, S, mask_c, ku, cfg, cap)
 
     step = None
+    prev_graph = None  # kept alive until the next capture has reused its pool
     wall = 0.0
     _sync(dev)
     t0 = time.perf_counter()
     for it in range(cfg.iterations):
         while True:
             if step is None or step.graph is None:
+                tc = time.perf_counter()
                 if step is None:
                     step = new_step()
                 step.eager()
@@ -457,8 +488,10 @@ def fit_graph(case: MRICase, init: GaussianSet, cfg: FitConfig, device="cuda:0",
                     st["overflows"] += 1
                     step = _GraphedStep(p, opt, vox, S, mask_c, ku, cfg, step.capacity * 2)
                     continue
-                step.capture()
+                step.capture(pool=prev_graph.pool() if prev_graph is not None else None)
+                prev_graph = step.graph
                 st["captures"] += 1
+                st["capture_seconds"] += time.perf_counter() - tc
                 break
             step.replay()
             if not step.overflowed():

@@ -152,6 +152,34 @@ GSV_API int gsv_backward(const gsv_params* params, gsv_shape shape, void* ws_gau
                  int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
                  void* stream);
 
+/* ---- batched persistent launches (many volumes, one launch) ---------- */
+
+/* No counterpart in the reference (the batched multi-volume launch is an
+ * addition).  One entry per volume, each already prepared and binned with
+ * gsv_prepare / gsv_bin into its own workspaces (tile edge 8). */
+typedef struct gsv_batch_item {
+    gsv_shape shape;
+    gsv_params params;        /* read by the backward (scales, rotations) */
+    const void* ws_gauss;
+    const void* ws_pairs;
+    int64_t capacity;
+    float* volume;            /* forward output, complex64 */
+    const float* grad_volume; /* backward input, complex64 */
+    gsv_grads grads;          /* backward outputs */
+} gsv_batch_item;
+
+GSV_API size_t gsv_batch_workspace_bytes(int count);
+/* Upload the descriptor table of `count` volumes into ws_batch (device);
+ * SYNCHRONISES the stream.  `flags`: GSV_BACKWARD_DETERMINISTIC must match
+ * the flags the pair workspaces were sized with. */
+GSV_API int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, void* ws_batch, size_t ws_bytes,
+                            void* stream);
+/* One persistent launch over every tile of every volume (CTAs pull tiles
+ * from an atomic counter); asynchronous, capturable. */
+GSV_API int gsv_forward_batched(void* ws_batch, int count, void* stream);
+/* Zeroing, one persistent backward launch, one finalize launch. */
+GSV_API int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream);
+
 /* ---- reference-compatible binning ------------------------------------ */
 
 /* build_tile_pairs(center_vox [n,3], radius_vox [n]) part 1: box + count +

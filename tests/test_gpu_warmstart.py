@@ -161,4 +161,6 @@ def test_full_time_to_nmse(cuda_device):
         with open(os.path.join(out, "warmstart_eval.json"), "w") as f:
             json.dump(report, f, indent=1)
     print(json.dumps({k: v for k, v in report.items() if k != "eval"}), json.dumps(rows))
-    assert all(r["warm_nmse_at_0"] < r["plain_nmse_at_0"] for r in rows)
+    # the plain method's final NMSE is reached, in at most half its wall time
+    assert all(r["warm_iterations_to_target"] is not None for r in rows)
+    assert report["median_wall_ratio"] <= 0.5
