@@ -87,21 +87,25 @@ def run_batched(args, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", 0))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    from gs_tmi_b200.autotune import WHOLE_TILE, Autotuner
+
     items = make_batch_inputs()
-    caps, evals = [], 0
+    caps, chunks, evals = [], [], 0
+    tuner = Autotuner()
     for shape, gs, _ in items:
         vz = TileVoxelizer(shape, device=str(dev))
         total = vz.count_pairs(gs.positions.to(dev), gs.scales.to(dev))
         caps.append(int(total * 1.1) + 1024)
-        plan = __import__("gs_tmi_b200").prepare_and_bin(tuple(t.to(dev) for t in gs.tensors()),
-                                                         vz._shape)
+        params = tuple(t.to(dev) for t in gs.tensors())
+        plan = __import__("gs_tmi_b200").prepare_and_bin(params, vz._shape)
+        chunks.append(32 if args.no_autotune else tuner.pick(plan, params, WHOLE_TILE).chunk)
         tr_ptr, _ = plan.views()
         nt = lib_num_tiles(vz._shape)
         off = tr_ptr - plan.ws_gauss.data_ptr()
         tr = plan.ws_gauss[off:off + 8 * nt].view(torch.int32).reshape(-1, 2).cpu().numpy()
         evals += evals_of(tr, shape)
     sb = batched.StaticBatch([s for s, _, _ in items], [gs.n for _, gs, _ in items], caps, device=str(dev),
-                             deterministic=args.deterministic)
+                             deterministic=args.deterministic, chunks=chunks)
     for i, (shape, gs, gv) in enumerate(items):
         for dst, src in zip(sb.params[i], gs.tensors()):
             dst.copy_(src.to(dev))
@@ -152,6 +156,7 @@ def run_batched(args, rank, world, dist):
            "dtype": "fp32", "data": "synthetic",
            "config": {"workload": "batch12", "volumes": [list(s) for s, _ in BATCH12],
                       "gaussians": [n for _, n in BATCH12], "tile_size": TILE, "evals_per_step": evals,
+                      "autotuned_chunk_per_volume": chunks,
                       "launch": "per-volume binning + 1 persistent forward + 1 persistent backward (+zero, "
                                 "finalize), one CUDA graph per iteration",
                       "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
@@ -339,12 +344,21 @@ def run_ours(args, rank, world, dist):
         check(lib.gsv_prepare(ctypes.byref(gp), gshape, wsg, plan.gauss_bytes, None, st), "prepare")
         check(lib.gsv_bin(gshape, n, wsg, wsp, plan.pair_bytes, cap, st), "bin")
 
+    tuning = None
+    if not args.no_autotune:
+        from gs_tmi_b200.autotune import Autotuner
+
+        tuner = Autotuner()
+        tuning = tuner.pick(plan, params)  # untimed: times every execution shape once
+        tune_times = next(iter(tuner.timings.values()), {})
+    tref = ctypes.byref(tuning) if tuning is not None else None
+
     def fwd():
-        check(lib.gsv_forward(gshape, n, wsg, wsp, cap, _ptr(vol), st), "forward")
+        check(lib.gsv_forward_ex(gshape, n, wsg, wsp, cap, _ptr(vol), tref, st), "forward")
 
     def bwd():
-        check(lib.gsv_backward(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags, st),
-              "backward")
+        check(lib.gsv_backward_ex(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags, tref,
+                                  st), "backward")
 
     def step():
         prep_bin()
@@ -398,7 +412,8 @@ def run_ours(args, rank, world, dist):
         raise RuntimeError(f"voxelizer status flags {fl} during the timed region")
 
     # e2e through the public module with pinned host buffers
-    vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic)
+    vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic,
+                        autotune=not args.no_autotune)
     host_in = [t.pin_memory() for t in gs.tensors()]
     gv_host = gv.pin_memory()
     host_out = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in gs.tensors()]
@@ -454,6 +469,8 @@ def run_ours(args, rank, world, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": name, "volume": list(shape), "gaussians": n, "tile_size": TILE, "pairs": total,
                    "evals_per_step": evals, "deterministic": bool(args.deterministic),
+                   "execution": ({"rows_per_lane": tuning.rows_per_lane, "chunk": tuning.chunk,
+                                  "autotune_ms_per_candidate": tune_times} if tuning is not None else "default"),
                    "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
         "breakdown_ms": {"prepare_bin": statistics.mean(t_bin), "forward": fwd_ms, "backward": bwd_ms},
         "roofline": {"bound": "fp32_issue", "kernel": "gsv_backward (k_backward8 + k_finalize)",
@@ -486,6 +503,7 @@ def main():
     ap.add_argument("--deterministic", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the CUDA activity trace (under ncu)")
+    ap.add_argument("--no-autotune", action="store_true", help="default execution shape, no tuning pass")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

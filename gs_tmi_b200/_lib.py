@@ -45,7 +45,11 @@ class GsvGrads(ctypes.Structure):
 class GsvBatchItem(ctypes.Structure):
     _fields_ = [("shape", GsvShape), ("params", GsvParams), ("ws_gauss", ctypes.c_void_p),
                 ("ws_pairs", ctypes.c_void_p), ("capacity", ctypes.c_int64), ("volume", ctypes.c_void_p),
-                ("grad_volume", ctypes.c_void_p), ("grads", GsvGrads)]
+                ("grad_volume", ctypes.c_void_p), ("grads", GsvGrads), ("chunk", ctypes.c_int32)]
+
+
+class GsvTuning(ctypes.Structure):
+    _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes); the complete exported C ABI.
@@ -66,6 +70,8 @@ SIGNATURES = {
     "gsv_status_views": (ctypes.c_int, [_S, _i64, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsv_read_status": (ctypes.c_int, [_S, _i64, _vp, _i64p, _i32p, _vp]),
     "gsv_forward": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, _vp, _vp]),
+    "gsv_forward_ex": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, _vp, ctypes.c_void_p, _vp]),
+    "gsv_backward_ex": (ctypes.c_int, [_P, _S, _vp, _vp, _i64, _vp, _G, ctypes.c_int, ctypes.c_void_p, _vp]),
     "gsv_backward": (ctypes.c_int, [_P, _S, _vp, _vp, _i64, _vp, _G, ctypes.c_int, _vp]),
     "gsv_batch_workspace_bytes": (_sz, [ctypes.c_int]),
     "gsv_batch_setup": (ctypes.c_int, [ctypes.POINTER(GsvBatchItem), ctypes.c_int, ctypes.c_int, _vp, _sz, _vp]),

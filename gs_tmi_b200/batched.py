@@ -24,12 +24,13 @@ from ._lib import GsvBatchItem, GsvGrads, GsvParams, check, lib
 from .tile_voxelizer import StaticPlan, _f32, _ptr, _shape, _stream, prepare_and_bin
 
 
-def _item(shape, params, plan, volume, grad_volume=None, grads=None) -> GsvBatchItem:
+def _item(shape, params, plan, volume, grad_volume=None, grads=None, chunk=32) -> GsvBatchItem:
     pos, scl, rot, dr, di = params
     gp = GsvParams(pos.data_ptr(), scl.data_ptr(), rot.data_ptr(), dr.data_ptr(), di.data_ptr(), plan.n)
     gg = GsvGrads(*(g.data_ptr() for g in grads)) if grads is not None else GsvGrads()
     return GsvBatchItem(shape, gp, plan.ws_gauss.data_ptr(), plan.ws_pairs.data_ptr(), plan.capacity,
-                        volume.data_ptr(), grad_volume.data_ptr() if grad_volume is not None else None, gg)
+                        volume.data_ptr(), grad_volume.data_ptr() if grad_volume is not None else None, gg,
+                        int(chunk))
 
 
 def _setup(items: List[GsvBatchItem], flags: int, device) -> torch.Tensor:
@@ -109,14 +110,15 @@ class StaticBatch:
     into ``params[i]`` and upstream gradients into ``grad_volumes[i]``;
     ``bin()``, ``forward()`` and ``backward()`` only enqueue work."""
 
-    def __init__(self, shapes, ns, capacities, device="cuda:0", deterministic: bool = False):
+    def __init__(self, shapes, ns, capacities, device="cuda:0", deterministic: bool = False, chunks=None):
         self.device = torch.device(device)
         self.flags = _lib.GSV_BACKWARD_DETERMINISTIC if deterministic else 0
         self.gshapes = [_shape(s, 8) for s in shapes]
         self.plans, self.params, self.volumes, self.grad_volumes, self.grads = [], [], [], [], []
         items = []
         dev = self.device
-        for shape, n, cap in zip(self.gshapes, ns, capacities):
+        chunks = chunks or [32] * len(self.gshapes)
+        for shape, n, cap, chunk in zip(self.gshapes, ns, capacities, chunks):
             plan = StaticPlan(shape, int(n), dev, int(cap), self.flags)
             params = [torch.zeros(n, 3, device=dev), torch.full((n, 3), 1e-2, device=dev),
                       torch.zeros(n, 4, device=dev), torch.zeros(n, device=dev), torch.zeros(n, device=dev)]
@@ -129,7 +131,7 @@ class StaticBatch:
             self.volumes.append(vol)
             self.grad_volumes.append(gvol)
             self.grads.append(grads)
-            items.append(_item(shape, params, plan, vol, gvol, grads))
+            items.append(_item(shape, params, plan, vol, gvol, grads, chunk))
         self.count = len(items)
         self.ws = _setup(items, self.flags, dev)
 

@@ -65,6 +65,7 @@ struct RenderArgs {
     float* g_cov;
     float* g_dr;
     float* g_di;
+    int chunk;  // Gaussians staged per warp chunk (<= 32)
     // finalize
     gsv_params prm;
     gsv_grads grd;
@@ -199,79 +200,87 @@ struct __align__(16) WarpStage {
     int32_t gid[32];
 };
 
+// Execution shape of a CTA on an 8^3 binning tile.  RPL (rows per lane) = 2:
+// the CTA covers the whole tile, lane l owns rows (d0+l/8, h0+l%8) and
+// (d0+4+l/8, h0+l%8).  RPL = 1: the CTA covers the 4x8x8 half `sub` of the
+// tile, lane l owns row (d0+4*sub+l/8, h0+l%8).  Either way each warp walks
+// its share of the tile's Gaussian list in chunks of `a.chunk` (<= 32).
 constexpr int kFwdSmem = kWarps * 16 * 32 * sizeof(float2);
 static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 
-// One 8^3 tile of the forward.  Contains two CTA barriers; every thread of
-// the CTA must call it for the same tile.
-template <bool COMPAT, bool PLANAR>
-__device__ __forceinline__ void forward_tile8(const RenderArgs& a, int64_t tile, unsigned char* smem_raw) {
+template <bool COMPAT>
+__device__ __forceinline__ void stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int w0,
+                                            const float ih[3]) {
+    if (lane < cnt) {
+        const int gid = __ldg(a.pair_ids + base + lane);
+        const Rec r = load_rec<COMPAT>(a, gid, ih);
+        S.rec[lane] = r;
+        S.gid[lane] = gid;
+        float e2[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
+        S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
+        S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
+    }
+}
+
+// Forward of one tile (RPL = 2) or half tile (RPL = 1).  Two CTA barriers:
+// every thread of the CTA must call it for the same (tile, sub).
+template <bool COMPAT, bool PLANAR, int RPL>
+__device__ __forceinline__ void forward_tile(const RenderArgs& a, int64_t tile, int sub, unsigned char* smem_raw) {
+    constexpr int NV = RPL * 8;  // voxels per lane
     WarpStage* stage = reinterpret_cast<WarpStage*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int d0, h0, w0;
     decode_tile(a, tile, d0, h0, w0);
     const int2 rg = a.ranges[tile];
+    const int chunk = a.chunk;
 
-    float accR[16], accI[16];
+    float accR[NV], accI[NV];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) accR[k] = accI[k] = 0.0f;
+    for (int k = 0; k < NV; ++k) accR[k] = accI[k] = 0.0f;
 
     if (rg.x < rg.y) {
         float ih[3];
         compat_ih<COMPAT>(a, ih);
-        const float ev0a = float(d0 + (lane >> 3));
-        const float ev0b = float(d0 + 4 + (lane >> 3));
+        float ev0[RPL];
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) ev0[r] = float(d0 + (lane >> 3) + 4 * (r + sub));
         const float ev1 = float(h0 + (lane & 7));
         WarpStage& S = stage[warp];
-        for (int base = rg.x + warp * 32; base < rg.y; base += kWarps * 32) {
-            const int cnt = min(32, rg.y - base);
-            if (lane < cnt) {
-                const int gid = __ldg(a.pair_ids + base + lane);
-                const Rec r = load_rec<COMPAT>(a, gid, ih);
-                S.rec[lane] = r;
-                float e2[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
-                S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
-                S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
-            }
+        for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
+            const int cnt = min(chunk, rg.y - base);
+            stage_chunk<COMPAT>(a, S, base, cnt, lane, w0, ih);
             __syncwarp();
             for (int j = 0; j < cnt; ++j) {
                 const Rec g = S.rec[j];
                 const float4 ea = S.e2[j][0], eb = S.e2[j][1];
                 const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
                 const float e1 = __fsub_rn(ev1, g.c1);
-                const float e0a = __fsub_rn(ev0a, g.c0);
-                const float e0b = __fsub_rn(ev0b, g.c0);
-                const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
-                const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
-                float m[16];
-                bool anyA = false, anyB = false;
+                float m[NV];
+                bool anyr[RPL];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    m[k] = row_m(g.q22, Aa, Ba, e2[k]);
-                    m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
-                    anyA |= (m[k] <= kCut);
-                    anyB |= (m[8 + k] <= kCut);
-                }
-                // the exp / FMA part of each half-tile runs only if some lane needs it
-                if (__any_sync(kFull, anyA)) {
+                for (int r = 0; r < RPL; ++r) {
+                    const float e0 = __fsub_rn(ev0[r], g.c0);
+                    const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
+                    anyr[r] = false;
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        if (m[k] <= kCut) {
-                            const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
-                            accR[k] = fmaf(wgt, g.rho_r, accR[k]);
-                            accI[k] = fmaf(wgt, g.rho_i, accI[k]);
-                        }
+                        m[r * 8 + k] = row_m(g.q22, A, B, e2[k]);
+                        anyr[r] |= (m[r * 8 + k] <= kCut);
                     }
                 }
-                if (__any_sync(kFull, anyB)) {
+                // the exp / FMA part of each row slot runs only if some lane needs it
 #pragma unroll
-                    for (int k = 8; k < 16; ++k) {
-                        if (m[k] <= kCut) {
-                            const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
-                            accR[k] = fmaf(wgt, g.rho_r, accR[k]);
-                            accI[k] = fmaf(wgt, g.rho_i, accI[k]);
+                for (int r = 0; r < RPL; ++r) {
+                    if (__any_sync(kFull, anyr[r])) {
+#pragma unroll
+                        for (int k = r * 8; k < r * 8 + 8; ++k) {
+                            if (m[k] <= kCut) {
+                                const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
+                                accR[k] = fmaf(wgt, g.rho_r, accR[k]);
+                                accI[k] = fmaf(wgt, g.rho_i, accI[k]);
+                            }
                         }
                     }
                 }
@@ -280,68 +289,75 @@ __device__ __forceinline__ void forward_tile8(const RenderArgs& a, int64_t tile,
         }
     }
 
-    // Sum the four warps' partial tiles: red[(warp*16 + k)*32 + lane].
+    // Sum the warps' partial (half) tiles: red[(warp*NV + k)*32 + lane].
     __syncthreads();
     float2* red = reinterpret_cast<float2*>(smem_raw);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) red[(warp * 16 + k) * 32 + lane] = make_float2(accR[k], accI[k]);
+    for (int k = 0; k < NV; ++k) red[(warp * NV + k) * 32 + lane] = make_float2(accR[k], accI[k]);
     __syncthreads();
 
-    // Thread t stores voxels 4t..4t+3 of the tile (row t/2, columns (t%2)*4..+3).
+    // Thread t stores VPT consecutive voxels of one row.
+    constexpr int VPT = 2 * RPL, TPR = 8 / VPT;
     const int t = threadIdx.x;
-    const int row = t >> 1;           // 0..63 = ld*8 + lh
-    const int ld = row >> 3, lh = row & 7, lw0 = (t & 1) * 4;
+    const int row = t / TPR;  // 0 .. 32*RPL-1
+    const int lw0 = (t % TPR) * VPT;
     const int src_lane = row & 31, slot = row >> 5;
-    float2 v[4];
+    float2 v[VPT];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < VPT; ++i) {
         const int k = slot * 8 + lw0 + i;
         float2 s = make_float2(0.f, 0.f);
 #pragma unroll
         for (int wv = 0; wv < kWarps; ++wv) {
-            const float2 x = red[(wv * 16 + k) * 32 + src_lane];
+            const float2 x = red[(wv * NV + k) * 32 + src_lane];
             s.x += x.x;
             s.y += x.y;
         }
         v[i] = s;
     }
-    const int gd = d0 + ld, gh = h0 + lh, gw = w0 + lw0;
+    const int gd = d0 + (src_lane >> 3) + 4 * (slot + sub), gh = h0 + (src_lane & 7), gw = w0 + lw0;
     if (gd >= a.d || gh >= a.h) return;
     const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
     if (PLANAR) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < VPT; ++i)
             if (gw + i < a.w) {
                 a.vol_r[flat + i] = v[i].x;
                 a.vol_i[flat + i] = v[i].y;
             }
     } else {
         float2* out = reinterpret_cast<float2*>(a.vol) + flat;
-        if (gw + 3 < a.w && (a.w & 1) == 0) {
+        if (gw + VPT - 1 < a.w && (a.w & 1) == 0) {
             float4* o4 = reinterpret_cast<float4*>(out);
-            o4[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
-            o4[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+#pragma unroll
+            for (int i = 0; i < VPT / 2; ++i)
+                o4[i] = make_float4(v[2 * i].x, v[2 * i].y, v[2 * i + 1].x, v[2 * i + 1].y);
         } else {
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < VPT; ++i)
                 if (gw + i < a.w) out[i] = v[i];
         }
     }
 }
 
-template <bool COMPAT, bool PLANAR>
+template <bool COMPAT, bool PLANAR, int RPL>
 __global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
     __shared__ __align__(16) unsigned char smem_raw[kFwdSmem];
-    forward_tile8<COMPAT, PLANAR>(a, blockIdx.x, smem_raw);
+    constexpr int subs = 2 / RPL;
+    forward_tile<COMPAT, PLANAR, RPL>(a, blockIdx.x / subs, blockIdx.x % subs, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
 // Tile edge 8: backward
 // ---------------------------------------------------------------------------
 
-// One 8^3 tile of the backward (warp-synchronous only, no CTA barrier).
-template <bool COMPAT, bool DET>
-__device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile, WarpStage* stage) {
+// Backward of one tile (RPL = 2) or half tile (RPL = 1); warp-synchronous
+// only.  The deterministic mode writes one partial per (tile, Gaussian) and
+// therefore runs with RPL = 2 only.
+template <bool COMPAT, bool DET, int RPL>
+__device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile, int sub, WarpStage* stage) {
+    static_assert(!DET || RPL == 2, "deterministic partials need the whole tile in one CTA");
+    constexpr int NV = RPL * 8;
     const int2 rg = a.ranges[tile];
     if (rg.x >= rg.y) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -349,14 +365,15 @@ __device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile
     decode_tile(a, tile, d0, h0, w0);
     float ih[3];
     compat_ih<COMPAT>(a, ih);
+    const int chunk = a.chunk;
 
-    // Upstream gradient of the lane's 16 voxels (zero outside the volume).
-    float gr[16], gi[16];
+    // Upstream gradient of the lane's voxels (zero outside the volume).
+    float gr[NV], gi[NV];
     {
         const int gh = h0 + (lane & 7);
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int gd = d0 + r * 4 + (lane >> 3);
+        for (int r = 0; r < RPL; ++r) {
+            const int gd = d0 + (lane >> 3) + 4 * (r + sub);
             const bool row_ok = gd < a.d && gh < a.h;
             const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + w0;
 #pragma unroll
@@ -375,50 +392,47 @@ __device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile
         }
     }
 
-    const float ev0a = float(d0 + (lane >> 3));
-    const float ev0b = float(d0 + 4 + (lane >> 3));
+    float ev0[RPL];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) ev0[r] = float(d0 + (lane >> 3) + 4 * (r + sub));
     const float ev1 = float(h0 + (lane & 7));
     WarpStage& S = stage[warp];
-    for (int base = rg.x + warp * 32; base < rg.y; base += kWarps * 32) {
-        const int cnt = min(32, rg.y - base);
-        if (lane < cnt) {
-            const int gid = __ldg(a.pair_ids + base + lane);
-            const Rec r = load_rec<COMPAT>(a, gid, ih);
-            S.rec[lane] = r;
-            S.gid[lane] = gid;
-            float e2[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
-            S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
-            S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
-        }
+    for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
+        const int cnt = min(chunk, rg.y - base);
+        stage_chunk<COMPAT>(a, S, base, cnt, lane, w0, ih);
         __syncwarp();
         for (int j = 0; j < cnt; ++j) {
             const Rec g = S.rec[j];
             const float4 ea = S.e2[j][0], eb = S.e2[j][1];
             const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
             const float e1 = __fsub_rn(ev1, g.c1);
-            const float e0a = __fsub_rn(ev0a, g.c0);
-            const float e0b = __fsub_rn(ev0b, g.c0);
-            const float Aa = row_a(g, e0a, e1), Ba = row_b(g, e0a, e1);
-            const float Ab = row_a(g, e0b, e1), Bb = row_b(g, e0b, e1);
-            float m[16];
-            bool anyA = false, anyB = false;
+            float m[NV], e0[RPL];
+            bool anyr[RPL];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                m[k] = row_m(g.q22, Aa, Ba, e2[k]);
-                m[8 + k] = row_m(g.q22, Ab, Bb, e2[k]);
-                anyA |= (m[k] <= kCut);
-                anyB |= (m[8 + k] <= kCut);
+            for (int r = 0; r < RPL; ++r) {
+                e0[r] = __fsub_rn(ev0[r], g.c0);
+                const float A = row_a(g, e0[r], e1), B = row_b(g, e0[r], e1);
+                anyr[r] = false;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    m[r * 8 + k] = row_m(g.q22, A, B, e2[k]);
+                    anyr[r] |= (m[r * 8 + k] <= kCut);
+                }
             }
-            const bool wA = __any_sync(kFull, anyA), wB = __any_sync(kFull, anyB);
-            if (!(wA || wB)) continue;
+            bool wr[RPL], wany = false;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                wr[r] = __any_sync(kFull, anyr[r]);
+                wany |= wr[r];
+            }
+            if (!wany) continue;
             const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
-            float R0[2] = {0.f, 0.f}, R1[2] = {0.f, 0.f}, R2[2] = {0.f, 0.f};
+            float R0[RPL], R1[RPL], R2[RPL];
             float Dr = 0.f, Di = 0.f;
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                if (!(r == 0 ? wA : wB)) continue;  // warp-uniform half-tile skip
+            for (int r = 0; r < RPL; ++r) {
+                R0[r] = R1[r] = R2[r] = 0.f;
+                if (!wr[r]) continue;  // warp-uniform row-slot skip
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int q = r * 8 + k;
@@ -435,18 +449,27 @@ __device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile
                 }
             }
             float v[16];
-            const float R0s = R0[0] + R0[1];
+            float R0s = 0.f, R1s = 0.f, R2s = 0.f, S1 = 0.f, S2 = 0.f, S3 = 0.f;
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                R0s += R0[r];
+                R1s += R1[r];
+                R2s += R2[r];
+                S1 = fmaf(e0[r], R0[r], S1);          // sum a e0
+                S2 = fmaf(e0[r] * e0[r], R0[r], S2);  // sum a e0^2
+                S3 = fmaf(e0[r], R1[r], S3);          // sum a e0 e2
+            }
             v[0] = Dr;
             v[1] = Di;
-            v[2] = fmaf(e0a, R0[0], e0b * R0[1]);
+            v[2] = S1;
             v[3] = e1 * R0s;
-            v[4] = R1[0] + R1[1];
-            v[5] = fmaf(e0a * e0a, R0[0], (e0b * e0b) * R0[1]);
-            v[6] = e1 * v[2];
-            v[7] = fmaf(e0a, R1[0], e0b * R1[1]);
+            v[4] = R1s;
+            v[5] = S2;
+            v[6] = e1 * S1;
+            v[7] = S3;
             v[8] = (e1 * e1) * R0s;
-            v[9] = e1 * v[4];
-            v[10] = R2[0] + R2[1];
+            v[9] = e1 * R1s;
+            v[10] = R2s;
 #pragma unroll
             for (int i = 11; i < 16; ++i) v[i] = 0.f;
             const float tot = warp_reduce_scatter16(v, lane);
@@ -465,10 +488,11 @@ __device__ __forceinline__ void backward_tile8(const RenderArgs& a, int64_t tile
     }
 }
 
-template <bool COMPAT, bool DET>
+template <bool COMPAT, bool DET, int RPL>
 __global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
     __shared__ __align__(16) WarpStage stage[kWarps];
-    backward_tile8<COMPAT, DET>(a, blockIdx.x, stage);
+    constexpr int subs = 2 / RPL;
+    backward_tile<COMPAT, DET, RPL>(a, blockIdx.x / subs, blockIdx.x % subs, stage);
 }
 
 // ---------------------------------------------------------------------------
@@ -760,7 +784,7 @@ __global__ void __launch_bounds__(kThreads) k_forward8_batched(const BatchTable 
         const int64_t gt = s_next;
         if (gt >= total) break;
         const int i = find_item(t.tile_prefix, t.count, gt);
-        forward_tile8<false, false>(t.items[i], gt - t.tile_prefix[i], smem_raw);
+        forward_tile<false, false, 2>(t.items[i], gt - t.tile_prefix[i], 0, smem_raw);
     }
 }
 
@@ -776,7 +800,7 @@ __global__ void __launch_bounds__(kThreads) k_backward8_batched(const BatchTable
         const int64_t gt = s_next;
         if (gt >= total) break;
         const int i = find_item(t.tile_prefix, t.count, gt);
-        backward_tile8<false, DET>(t.items[i], gt - t.tile_prefix[i], stage);
+        backward_tile<false, DET, 2>(t.items[i], gt - t.tile_prefix[i], 0, stage);
     }
 }
 
@@ -823,6 +847,7 @@ void fill_shape(RenderArgs& a, gsv_shape s) {
     a.nth = (s.h + s.tile_size - 1) / s.tile_size;
     a.ntw = (s.w + s.tile_size - 1) / s.tile_size;
     a.ntiles = int64_t((s.d + s.tile_size - 1) / s.tile_size) * a.nth * a.ntw;
+    a.chunk = 32;
     const float sh[3] = {float(s.d), float(s.h), float(s.w)};
     for (int k = 0; k < 3; ++k) {
         a.hs[k] = sh[k] * 0.5f;
@@ -840,6 +865,16 @@ extern "C" {
 
 int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,
                 int64_t capacity, float* volume, void* stream) {
+    return gsv_forward_ex(shape, n, ws_gauss, ws_pairs, capacity, volume, nullptr, stream);
+}
+
+static bool tuning_ok(const gsv_tuning* t) {
+    return !t || ((t->rows_per_lane == 1 || t->rows_per_lane == 2) && t->chunk >= 1 && t->chunk <= 32);
+}
+
+int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs, int64_t capacity,
+                   float* volume, const gsv_tuning* tuning, void* stream) {
+    if (!tuning_ok(tuning)) return GSV_ERR_INVALID_ARGUMENT;
     GaussLayout G;
     PairLayout P;
     int64_t ntiles = 0;
@@ -854,7 +889,10 @@ int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws
     a.ranges = cat<int2>(ws_gauss, G.ranges);
     a.pair_ids = capacity > 0 ? cat<int32_t>(ws_pairs, P.vals_out) : nullptr;
     a.vol = volume;
-    if (shape.tile_size == 8) k_forward8<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+    const int rpl = tuning ? tuning->rows_per_lane : 2;
+    if (tuning) a.chunk = tuning->chunk;
+    if (shape.tile_size == 8 && rpl == 2) k_forward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+    else if (shape.tile_size == 8) k_forward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
     else k_forward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
@@ -863,6 +901,13 @@ int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws
 int gsv_backward(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* ws_pairs,
                  int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
                  void* stream) {
+    return gsv_backward_ex(p, shape, ws_gauss, ws_pairs, capacity, grad_volume, grads, flags, nullptr, stream);
+}
+
+int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* ws_pairs, int64_t capacity,
+                    const float* grad_volume, const gsv_grads* grads, int flags, const gsv_tuning* tuning,
+                    void* stream) {
+    if (!tuning_ok(tuning)) return GSV_ERR_INVALID_ARGUMENT;
     GaussLayout G;
     PairLayout P;
     int64_t ntiles = 0;
@@ -890,10 +935,13 @@ int gsv_backward(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* ws_
     } else {
         GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
     }
+    if (tuning) a.chunk = tuning->chunk;
+    const int rpl = (tuning && !det) ? tuning->rows_per_lane : 2;  // deterministic: whole tiles
     if (capacity > 0) {
         if (shape.tile_size == 8) {
-            if (det) k_backward8<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
-            else k_backward8<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            if (det) k_backward8<false, true, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            else if (rpl == 2) k_backward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            else k_backward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
         } else {
             if (det) k_backward_generic<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
             else k_backward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
@@ -930,7 +978,7 @@ int gsv_tile_forward(const float* centers, const float* cov_inv, const float* de
     a.vol_r = vol_r;
     a.vol_i = vol_i;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (tile_size == 8) k_forward8<true, true><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    if (tile_size == 8) k_forward8<true, true, 2><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     else k_forward_generic<true, true><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
@@ -971,7 +1019,7 @@ int gsv_tile_backward(const float* centers, const float* cov_inv, const float* d
     a.g_cov = grad_cov_inv;
     a.g_dr = grad_den_r;
     a.g_di = grad_den_i;
-    if (tile_size == 8) k_backward8<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    if (tile_size == 8) k_backward8<true, false, 2><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     else k_backward_generic<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
@@ -1015,6 +1063,7 @@ int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, void* ws_
         a.prm = it.params;
         a.grd = it.grads;
         a.boxes = cat<int4>(it.ws_gauss, G.box);
+        a.chunk = (it.chunk >= 1 && it.chunk <= 32) ? it.chunk : 32;
         host[i] = a;
         tp[i + 1] = tp[i] + ntiles;
         gp[i + 1] = gp[i] + it.params.n;

@@ -133,15 +133,16 @@ class _VoxelizeFn(torch.autograd.Function):
     the autograd tail through :284-290 and :77-84, all in the library."""
 
     @staticmethod
-    def forward(ctx, positions, scales, rotations, density_r, density_i, shape, deterministic):
+    def forward(ctx, positions, scales, rotations, density_r, density_i, shape, deterministic, tuner=None):
         params = tuple(_f32(t) for t in (positions, scales, rotations, density_r, density_i))
         dev = _require_cuda(*params)
         flags = _lib.GSV_BACKWARD_DETERMINISTIC if deterministic else 0
         with torch.cuda.device(dev):
             plan = prepare_and_bin(params, shape, flags)
+            plan.tuning = tuner.pick(plan, params) if tuner is not None else None
             vol = torch.empty((shape.d, shape.h, shape.w), dtype=torch.complex64, device=dev)
-            check(lib.gsv_forward(shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
-                                  _ptr(vol), _stream(dev)), "gsv_forward")
+            check(lib.gsv_forward_ex(shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
+                                     _ptr(vol), _tuning_ref(plan), _stream(dev)), "gsv_forward")
         ctx.plan = plan
         ctx.save_for_backward(*params)
         return vol
@@ -155,16 +156,21 @@ class _VoxelizeFn(torch.autograd.Function):
         outs = [torch.empty_like(t) for t in params]
         with torch.cuda.device(dev):
             backward_into(plan, params, g, outs)
-        return (*outs, None, None)
+        return (*outs, None, None, None)
+
+
+def _tuning_ref(plan):
+    t = getattr(plan, "tuning", None)
+    return ctypes.byref(t) if t is not None else None
 
 
 def backward_into(plan: BinPlan, params, grad_vol: torch.Tensor, outs) -> None:
     pos, scl, rot, dr, di = params
     gp = GsvParams(pos.data_ptr(), scl.data_ptr(), rot.data_ptr(), dr.data_ptr(), di.data_ptr(), plan.n)
     gg = GsvGrads(*(o.data_ptr() for o in outs))
-    check(lib.gsv_backward(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs),
-                           plan.capacity, _ptr(grad_vol), ctypes.byref(gg), plan.flags,
-                           _stream(plan.device)), "gsv_backward")
+    check(lib.gsv_backward_ex(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs),
+                              plan.capacity, _ptr(grad_vol), ctypes.byref(gg), plan.flags, _tuning_ref(plan),
+                              _stream(plan.device)), "gsv_backward")
 
 
 class StaticPlan(BinPlan):
@@ -219,11 +225,12 @@ class _VoxelizeStaticFn(torch.autograd.Function):
 
 def voxelize(positions: torch.Tensor, scales: torch.Tensor, rotations: torch.Tensor,
              density_r: torch.Tensor, density_i: torch.Tensor, volume_shape, tile_size: int = 8,
-             deterministic: bool = False) -> torch.Tensor:
+             deterministic: bool = False, tuner=None) -> torch.Tensor:
     """Functional form: complex64 (D,H,W) volume, differentiable in all five
-    parameter tensors."""
+    parameter tensors.  `tuner`: an autotune.Autotuner picking the execution
+    shape (results do not depend on it)."""
     return _VoxelizeFn.apply(positions, scales, rotations, density_r, density_i,
-                             _shape(volume_shape, tile_size), bool(deterministic))
+                             _shape(volume_shape, tile_size), bool(deterministic), tuner)
 
 
 # ---------------------------------------------------------------------------
@@ -308,11 +315,13 @@ class TileVoxelizer(nn.Module):
     ``"tile_cuda"``; ``use_cuda=False`` or a machine without CUDA raises
     instead of falling back to a CPU path.  ``max_radius`` is stored and
     unused, as in the reference.  ``deterministic=True`` selects the
-    fixed-order backward (bitwise reproducible gradients)."""
+    fixed-order backward (bitwise reproducible gradients); ``autotune=True``
+    lets the project autotuner pick the execution tile shape and Gaussian
+    batch per (volume, Gaussian-count bucket) -- results do not change."""
 
     def __init__(self, volume_shape: Tuple[int, int, int], tile_size: int = 8, max_radius: int = 20,
                  use_cuda: bool = True, strict_cuda: bool = False, device: str = "cuda:0",
-                 deterministic: bool = False):
+                 deterministic: bool = False, autotune: bool = False):
         super().__init__()
         self.volume_shape = tuple(int(x) for x in volume_shape)
         self.tile_size = int(tile_size)
@@ -327,6 +336,11 @@ class TileVoxelizer(nn.Module):
         self.use_cuda = True
         self.backend = "tile_cuda"
         self._shape = _shape(self.volume_shape, self.tile_size)
+        self.tuner = None
+        if autotune:
+            from .autotune import default_tuner
+
+            self.tuner = default_tuner()
 
     def forward(self, positions: torch.Tensor, scales: torch.Tensor, rotations: torch.Tensor,
                 density: torch.Tensor, chunk_size: int = 4096) -> torch.Tensor:
@@ -335,7 +349,7 @@ class TileVoxelizer(nn.Module):
             dr, di = density.real, density.imag
         else:
             dr, di = density, torch.zeros_like(density)
-        return _VoxelizeFn.apply(positions, scales, rotations, dr, di, self._shape, self.deterministic)
+        return _VoxelizeFn.apply(positions, scales, rotations, dr, di, self._shape, self.deterministic, self.tuner)
 
     def static(self, n: int, capacity: int) -> "StaticVoxelizer":
         """A sync-free, allocation-free variant for `n` Gaussians and at most

@@ -166,6 +166,7 @@ typedef struct gsv_batch_item {
     float* volume;            /* forward output, complex64 */
     const float* grad_volume; /* backward input, complex64 */
     gsv_grads grads;          /* backward outputs */
+    int32_t chunk;            /* Gaussians per warp chunk, 1..32 (0 = 32) */
 } gsv_batch_item;
 
 GSV_API size_t gsv_batch_workspace_bytes(int count);
@@ -179,6 +180,26 @@ GSV_API int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, v
 GSV_API int gsv_forward_batched(void* ws_batch, int count, void* stream);
 /* Zeroing, one persistent backward launch, one finalize launch. */
 GSV_API int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream);
+
+/* ---- execution tuning (results do not depend on it) ------------------ */
+
+/* No counterpart in the reference.  rows_per_lane: 2 = one CTA per 8^3 tile
+ * (two 8-voxel rows per lane), 1 = one CTA per 4x8x8 half tile (one row per
+ * lane; the deterministic backward always uses whole tiles).  chunk: number
+ * of Gaussians a warp stages in shared memory at a time (1..32).  Tile edge 8
+ * only; other tile edges ignore it. */
+typedef struct gsv_tuning {
+    int32_t rows_per_lane;
+    int32_t chunk;
+} gsv_tuning;
+
+/* gsv_forward / gsv_backward with an explicit execution shape (NULL =
+ * defaults: rows_per_lane 2, chunk 32). */
+GSV_API int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,
+                           int64_t capacity, float* volume, const gsv_tuning* tuning, void* stream);
+GSV_API int gsv_backward_ex(const gsv_params* params, gsv_shape shape, void* ws_gauss, void* ws_pairs,
+                            int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
+                            const gsv_tuning* tuning, void* stream);
 
 /* ---- reference-compatible binning ------------------------------------ */
 

@@ -1,0 +1,71 @@
+"""The execution shapes the autotuner chooses between give the same results
+(against the FP64 oracle; whole-tile and half-tile forwards with the same
+Gaussian batch are bitwise equal), and the tuner caches its pick."""
+import ctypes
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from gs_tmi_b200 import autotune, synthetic
+from gs_tmi_b200._lib import GsvGrads, GsvParams, GsvTuning, check, lib
+from gs_tmi_b200.tile_voxelizer import _ptr, _shape, prepare_and_bin
+from oracle import oracle as O
+from tests.helpers import FWD_TOL, GRAD_TOL, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(plan, params, gv, tun):
+    dev = plan.device
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    vol = torch.empty((plan.shape.d, plan.shape.h, plan.shape.w), dtype=torch.complex64, device=dev)
+    outs = [torch.empty_like(t) for t in params]
+    check(lib.gsv_forward_ex(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity, _ptr(vol),
+                             ctypes.byref(tun), st), "fwd")
+    gp = GsvParams(*(t.data_ptr() for t in params), plan.n)
+    gg = GsvGrads(*(o.data_ptr() for o in outs))
+    check(lib.gsv_backward_ex(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
+                              _ptr(gv), ctypes.byref(gg), plan.flags, ctypes.byref(tun), st), "bwd")
+    torch.cuda.synchronize(dev)
+    return vol.cpu().numpy(), [o.cpu().numpy() for o in outs]
+
+
+@pytest.mark.parametrize("shape", [(40, 48, 32), (37, 29, 45)])
+def test_candidates_agree_with_oracle(shape, cuda_device):
+    gs = synthetic.random_gaussians(3000, shape, seed=61)
+    gv = synthetic.upstream_grad(shape, seed=62)
+    params = tuple(t.to(cuda_device) for t in gs.tensors())
+    plan = prepare_and_bin(params, _shape(shape, 8))
+    p = tuple(t.numpy() for t in gs.tensors())
+    c, r, _ = O.preprocess_f32(*p[:3], shape)
+    tr, pid = O.build_tile_pairs(c, r, shape, 8)
+    ovol, _ = O.forward(p, shape, 8, tr, pid)
+    og = O.backward(p, shape, 8, tr, pid, gv.numpy())
+    vols = {}
+    for rpl, chunk in autotune.CANDIDATES:
+        vol, grads = _run(plan, params, gv.to(cuda_device), GsvTuning(rpl, chunk))
+        vols[(rpl, chunk)] = vol
+        assert rel(vol, ovol) < FWD_TOL
+        for a, b in zip(grads, og):
+            assert rel(a, b) < GRAD_TOL
+    assert np.array_equal(vols[(2, 32)], vols[(1, 32)])
+    assert np.array_equal(vols[(2, 16)], vols[(1, 16)])
+
+
+def test_tuner_picks_and_caches(tmp_path, cuda_device):
+    shape = (64, 64, 64)
+    gs = synthetic.random_gaussians(20000, shape, seed=0)
+    params = tuple(t.to(cuda_device) for t in gs.tensors())
+    plan = prepare_and_bin(params, _shape(shape, 8))
+    path = tmp_path / "tune.json"
+    tuner = autotune.Autotuner(str(path))
+    t1 = tuner.pick(plan, params)
+    assert (t1.rows_per_lane, t1.chunk) in autotune.CANDIDATES
+    k = autotune.Autotuner.key(plan.shape, plan.n, False)
+    assert len(tuner.timings[k]) == len(autotune.CANDIDATES)
+    again = autotune.Autotuner(str(path))
+    t2 = again.pick(plan, params)
+    assert (t2.rows_per_lane, t2.chunk) == (t1.rows_per_lane, t1.chunk) and not again.timings
+    assert json.loads(path.read_text())[k] == [t1.rows_per_lane, t1.chunk]
