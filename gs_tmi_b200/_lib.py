@@ -23,6 +23,7 @@ GSV_FLAG_EMPTY_BOX = 0x2
 GSV_FLAG_TOO_MANY_PAIRS = 0x4
 
 GSV_BACKWARD_DETERMINISTIC = 0x1
+GSV_TUNE_NO_CULL = 0x1
 
 
 class GsvShape(ctypes.Structure):
@@ -49,7 +50,7 @@ class GsvBatchItem(ctypes.Structure):
 
 
 class GsvTuning(ctypes.Structure):
-    _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32)]
+    _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes); the complete exported C ABI.

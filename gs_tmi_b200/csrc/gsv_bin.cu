@@ -60,6 +60,7 @@ GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
     L.scan_tmp_bytes = scan_bytes;
     size_t o = 0;
     L.rec = o;      o = align_up(o + size_t(n) * sizeof(Rec));
+    L.ext = o;      o = align_up(o + size_t(n) * sizeof(float4));
     L.box = o;      o = align_up(o + size_t(n) * sizeof(int4));
     L.counts = o;   o = align_up(o + size_t(n + 1) * sizeof(int64_t));
     L.offsets = o;  o = align_up(o + size_t(n + 1) * sizeof(int64_t));
@@ -158,7 +159,8 @@ __global__ void __launch_bounds__(256) k_prepare(const float* __restrict__ pos,
                                                  const float* __restrict__ rot,
                                                  const float* __restrict__ dr,
                                                  const float* __restrict__ di, int64_t n, DevShape s,
-                                                 Rec* __restrict__ recs, int4* __restrict__ boxes,
+                                                 Rec* __restrict__ recs, float4* __restrict__ ext,
+                                                 int4* __restrict__ boxes,
                                                  int64_t* __restrict__ counts, Status* status) {
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g == 0) counts[n] = 0;
@@ -186,6 +188,7 @@ __global__ void __launch_bounds__(256) k_prepare(const float* __restrict__ pos,
     R.q00 = qc[0]; R.q01x2 = qc[1]; R.q02x2 = qc[2]; R.q11 = qc[3]; R.q12x2 = qc[4]; R.q22 = qc[5];
     R.rho_r = dr[g]; R.rho_i = di[g]; R.pad = 0.0f;
     recs[g] = R;
+    ext[g] = tight_extent(qc);
     int4 box;
     int64_t cnt = tile_box(s, c, r, &box);
     if (cnt <= 0) {
@@ -383,6 +386,7 @@ int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_
     GSV_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(Status), st));
     k_prepare<<<grid_for(n + 1, 256), 256, 0, st>>>(p->positions, p->scales, p->rotations, p->density_r,
                                                     p->density_i, n, dev_shape(si), at<Rec>(ws_gauss, L.rec),
+                                                    at<float4>(ws_gauss, L.ext),
                                                     at<int4>(ws_gauss, L.box), at<int64_t>(ws_gauss, L.counts),
                                                     status);
     GSV_LAUNCH_CHECK();

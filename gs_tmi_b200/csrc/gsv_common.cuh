@@ -105,6 +105,36 @@ __device__ __forceinline__ void qcoef_from_covinv(const float* m9, const float i
     }
 }
 
+// Conservative tight extent of the inclusion set {e : m_fp32(e) <= 9}.
+//
+// For the exact quadratic form of the stored FP32 coefficients, m(e) <= 9
+// implies |e_a| <= 3 sqrt(S_aa) with S = Q^-1 (Schur complement bound).  The
+// FP32 row evaluation used by the kernels differs from the exact form by at
+// most ~6 u sum_ab |Q_ab e_a e_b| <= ~3e-5 K (u = 2^-24), where
+// K = max_a Q_aa S_aa >= 1 measures anisotropy, so m_fp32 <= 9 implies
+// m <= 9 (1 + 3.3e-6 K).  The extent is widened by a factor
+// sqrt(1 + 1e-4 K) (30x that bound) plus 0.01 voxel for the FP32 rounding
+// of c -/+ extent at the culling site.  Q not positive definite, NaN, or
+// K > 1e4: infinite extent (nothing is culled).  Computed in FP64 from the
+// stored coefficients, rounded up.
+__device__ __forceinline__ float4 tight_extent(const float qc[6]) {
+    const double q00 = qc[0], q01 = 0.5 * double(qc[1]), q02 = 0.5 * double(qc[2]);
+    const double q11 = qc[3], q12 = 0.5 * double(qc[4]), q22 = qc[5];
+    const double c00 = q11 * q22 - q12 * q12, c11 = q00 * q22 - q02 * q02, c22 = q00 * q11 - q01 * q01;
+    const double c01 = q02 * q12 - q01 * q22, c02 = q01 * q12 - q02 * q11;
+    const double det = q00 * c00 + q01 * c01 + q02 * c02;
+    const float inf = __int_as_float(0x7f800000);
+    if (!(q00 > 0.0 && c22 > 0.0 && det > 0.0 && c00 > 0.0 && c11 > 0.0)) return make_float4(inf, inf, inf, 0.f);
+    const double s0 = c00 / det, s1 = c11 / det, s2 = c22 / det;
+    double k = q00 * s0;
+    k = fmax(k, q11 * s1);
+    k = fmax(k, q22 * s2);
+    if (!(k <= 1e4)) return make_float4(inf, inf, inf, 0.f);
+    const double f = 9.0 * (1.0 + 1e-4 * k);
+    return make_float4(__double2float_ru(sqrt(f * s0) + 0.01), __double2float_ru(sqrt(f * s1) + 0.01),
+                       __double2float_ru(sqrt(f * s2) + 0.01), 0.f);
+}
+
 // Row terms of the quadratic form for fixed (e0, e1):
 //   m(e2) = fma(fma(q22, e2, B), e2, A)
 __device__ __forceinline__ float row_a(const Rec& g, float e0, float e1) {
@@ -125,7 +155,7 @@ __device__ __forceinline__ float row_m(float q22, float a, float b, float e2) {
 __host__ __device__ inline size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct GaussLayout {
-    size_t rec, box, counts, offsets, scan_tmp, ranges, accum, status, total;
+    size_t rec, ext, box, counts, offsets, scan_tmp, ranges, accum, status, total;
     size_t scan_tmp_bytes;
 };
 

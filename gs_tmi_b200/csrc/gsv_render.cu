@@ -39,6 +39,7 @@ constexpr int kThreads = kWarps * 32;
 struct RenderArgs {
     // native Gaussians
     const Rec* recs;
+    const float4* ext;  // conservative tight extent of each inclusion set (voxels)
     // reference-compatible Gaussians
     const float* centers;
     const float* cov_inv;
@@ -66,6 +67,7 @@ struct RenderArgs {
     float* g_dr;
     float* g_di;
     int chunk;  // Gaussians staged per warp chunk (<= 32)
+    int cull;   // skip Gaussians / row slots outside the tight extent
     // finalize
     gsv_params prm;
     gsv_grads grd;
@@ -198,6 +200,7 @@ struct __align__(16) WarpStage {
     Rec rec[32];
     float4 e2[32][2];
     int32_t gid[32];
+    int32_t meta[32];  // bit r: row slot r may hold included voxels; bits 8+: position in the chunk
 };
 
 // Execution shape of a CTA on an 8^3 binning tile.  RPL (rows per lane) = 2:
@@ -208,20 +211,47 @@ struct __align__(16) WarpStage {
 constexpr int kFwdSmem = kWarps * 16 * 32 * sizeof(float2);
 static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 
-template <bool COMPAT>
-__device__ __forceinline__ void stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int w0,
-                                            const float ih[3]) {
+// Stages Gaussians [base, base + cnt) of the tile list and returns how many
+// were kept.  Native layout: a Gaussian is kept only if its conservative
+// tight extent (Rec + ext, see tight_extent) reaches the CTA's rows, and it
+// carries one bit per row slot it reaches; a dropped Gaussian or slot has
+// m > 9 at every voxel there, so skipping it changes no sum.  The kept
+// Gaussians keep their list order.  Compat layout: everything is kept.
+template <bool COMPAT, int RPL>
+__device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int d0,
+                                           int h0, int w0, int sub, const float ih[3]) {
+    Rec r;
+    int gid = 0, bits = 0;
     if (lane < cnt) {
-        const int gid = __ldg(a.pair_ids + base + lane);
-        const Rec r = load_rec<COMPAT>(a, gid, ih);
-        S.rec[lane] = r;
-        S.gid[lane] = gid;
+        gid = __ldg(a.pair_ids + base + lane);
+        r = load_rec<COMPAT>(a, gid, ih);
+        if (COMPAT || !a.cull) {
+            bits = (1 << RPL) - 1;
+        } else {
+            const float4 x = __ldg(a.ext + gid);
+            const bool hw = __fsub_rn(r.c1, x.y) <= float(h0 + 7) && __fadd_rn(r.c1, x.y) >= float(h0) &&
+                            __fsub_rn(r.c2, x.z) <= float(w0 + 7) && __fadd_rn(r.c2, x.z) >= float(w0);
+            const float lo = __fsub_rn(r.c0, x.x), hi = __fadd_rn(r.c0, x.x);
+#pragma unroll
+            for (int k = 0; k < RPL; ++k) {
+                const int ds = d0 + 4 * (k + sub);
+                if (hw && lo <= float(ds + 3) && hi >= float(ds)) bits |= 1 << k;
+            }
+        }
+    }
+    const unsigned keep = __ballot_sync(kFull, bits != 0);
+    if (bits) {
+        const int pos = __popc(keep & ((1u << lane) - 1u));
+        S.rec[pos] = r;
+        S.gid[pos] = gid;
+        S.meta[pos] = bits | (lane << 8);
         float e2[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
-        S.e2[lane][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
-        S.e2[lane][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
+        S.e2[pos][0] = make_float4(e2[0], e2[1], e2[2], e2[3]);
+        S.e2[pos][1] = make_float4(e2[4], e2[5], e2[6], e2[7]);
     }
+    return __popc(keep);
 }
 
 // Forward of one tile (RPL = 2) or half tile (RPL = 1).  Two CTA barriers:
@@ -249,37 +279,34 @@ __device__ __forceinline__ void forward_tile(const RenderArgs& a, int64_t tile, 
         const float ev1 = float(h0 + (lane & 7));
         WarpStage& S = stage[warp];
         for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
-            const int cnt = min(chunk, rg.y - base);
-            stage_chunk<COMPAT>(a, S, base, cnt, lane, w0, ih);
+            const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, rg.y - base), lane, d0, h0, w0, sub, ih);
             __syncwarp();
-            for (int j = 0; j < cnt; ++j) {
+            for (int j = 0; j < kept; ++j) {
                 const Rec g = S.rec[j];
+                const int bits = S.meta[j];  // warp-uniform
                 const float4 ea = S.e2[j][0], eb = S.e2[j][1];
                 const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
                 const float e1 = __fsub_rn(ev1, g.c1);
-                float m[NV];
-                bool anyr[RPL];
 #pragma unroll
                 for (int r = 0; r < RPL; ++r) {
+                    if (!(bits & (1 << r))) continue;  // slot out of the Gaussian's extent
                     const float e0 = __fsub_rn(ev0[r], g.c0);
                     const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
-                    anyr[r] = false;
+                    float m[8];
+                    bool any = false;
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        m[r * 8 + k] = row_m(g.q22, A, B, e2[k]);
-                        anyr[r] |= (m[r * 8 + k] <= kCut);
+                        m[k] = row_m(g.q22, A, B, e2[k]);
+                        any |= (m[k] <= kCut);
                     }
-                }
-                // the exp / FMA part of each row slot runs only if some lane needs it
+                    // the exp / FMA part of the slot runs only if some lane needs it
+                    if (__any_sync(kFull, any)) {
 #pragma unroll
-                for (int r = 0; r < RPL; ++r) {
-                    if (__any_sync(kFull, anyr[r])) {
-#pragma unroll
-                        for (int k = r * 8; k < r * 8 + 8; ++k) {
+                        for (int k = 0; k < 8; ++k) {
                             if (m[k] <= kCut) {
                                 const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
-                                accR[k] = fmaf(wgt, g.rho_r, accR[k]);
-                                accI[k] = fmaf(wgt, g.rho_i, accI[k]);
+                                accR[r * 8 + k] = fmaf(wgt, g.rho_r, accR[r * 8 + k]);
+                                accI[r * 8 + k] = fmaf(wgt, g.rho_i, accI[r * 8 + k]);
                             }
                         }
                     }
@@ -398,46 +425,38 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
     const float ev1 = float(h0 + (lane & 7));
     WarpStage& S = stage[warp];
     for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
-        const int cnt = min(chunk, rg.y - base);
-        stage_chunk<COMPAT>(a, S, base, cnt, lane, w0, ih);
+        const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, rg.y - base), lane, d0, h0, w0, sub, ih);
         __syncwarp();
-        for (int j = 0; j < cnt; ++j) {
+        for (int j = 0; j < kept; ++j) {
             const Rec g = S.rec[j];
+            const int bits = S.meta[j];  // warp-uniform
             const float4 ea = S.e2[j][0], eb = S.e2[j][1];
             const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
             const float e1 = __fsub_rn(ev1, g.c1);
-            float m[NV], e0[RPL];
-            bool anyr[RPL];
+            const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
+            float e0[RPL], R0[RPL], R1[RPL], R2[RPL];
+            float Dr = 0.f, Di = 0.f;
+            bool wany = false;
 #pragma unroll
             for (int r = 0; r < RPL; ++r) {
                 e0[r] = __fsub_rn(ev0[r], g.c0);
+                R0[r] = R1[r] = R2[r] = 0.f;
+                if (!(bits & (1 << r))) continue;  // slot out of the Gaussian's extent
                 const float A = row_a(g, e0[r], e1), B = row_b(g, e0[r], e1);
-                anyr[r] = false;
+                float m[8];
+                bool any = false;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    m[r * 8 + k] = row_m(g.q22, A, B, e2[k]);
-                    anyr[r] |= (m[r * 8 + k] <= kCut);
+                    m[k] = row_m(g.q22, A, B, e2[k]);
+                    any |= (m[k] <= kCut);
                 }
-            }
-            bool wr[RPL], wany = false;
-#pragma unroll
-            for (int r = 0; r < RPL; ++r) {
-                wr[r] = __any_sync(kFull, anyr[r]);
-                wany |= wr[r];
-            }
-            if (!wany) continue;
-            const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
-            float R0[RPL], R1[RPL], R2[RPL];
-            float Dr = 0.f, Di = 0.f;
-#pragma unroll
-            for (int r = 0; r < RPL; ++r) {
-                R0[r] = R1[r] = R2[r] = 0.f;
-                if (!wr[r]) continue;  // warp-uniform row-slot skip
+                if (!__any_sync(kFull, any)) continue;  // warp-uniform row-slot skip
+                wany = true;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int q = r * 8 + k;
-                    if (m[q] <= kCut) {
-                        const float wgt = ex2_approx(m[q] * kNegHalfLog2e);
+                    if (m[k] <= kCut) {
+                        const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
                         const float av = wgt * fmaf(hi, gi[q], hr * gr[q]);
                         Dr = fmaf(wgt, gr[q], Dr);
                         Di = fmaf(wgt, gi[q], Di);
@@ -448,6 +467,7 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                     }
                 }
             }
+            if (!wany) continue;
             float v[16];
             float R0s = 0.f, R1s = 0.f, R2s = 0.f, S1 = 0.f, S2 = 0.f, S3 = 0.f;
 #pragma unroll
@@ -478,7 +498,7 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                 compat_emit(a, g, gid, tot, lane, ih);
             } else if (DET) {
                 if (!(lane & 1) && (lane >> 1) < kMom)
-                    a.partials[int64_t(base + j) * kMomStride + (lane >> 1)] = tot;
+                    a.partials[int64_t(base + (bits >> 8)) * kMomStride + (lane >> 1)] = tot;
             } else {
                 if (!(lane & 1) && (lane >> 1) < kMom)
                     atomicAdd(a.accum + int64_t(gid) * kMomStride + (lane >> 1), tot);
@@ -848,6 +868,7 @@ void fill_shape(RenderArgs& a, gsv_shape s) {
     a.ntw = (s.w + s.tile_size - 1) / s.tile_size;
     a.ntiles = int64_t((s.d + s.tile_size - 1) / s.tile_size) * a.nth * a.ntw;
     a.chunk = 32;
+    a.cull = 1;
     const float sh[3] = {float(s.d), float(s.h), float(s.w)};
     for (int k = 0; k < 3; ++k) {
         a.hs[k] = sh[k] * 0.5f;
@@ -886,11 +907,15 @@ int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void*
     RenderArgs a{};
     fill_shape(a, shape);
     a.recs = cat<Rec>(ws_gauss, G.rec);
+    a.ext = cat<float4>(ws_gauss, G.ext);
     a.ranges = cat<int2>(ws_gauss, G.ranges);
     a.pair_ids = capacity > 0 ? cat<int32_t>(ws_pairs, P.vals_out) : nullptr;
     a.vol = volume;
     const int rpl = tuning ? tuning->rows_per_lane : 2;
-    if (tuning) a.chunk = tuning->chunk;
+    if (tuning) {
+        a.chunk = tuning->chunk;
+        a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
+    }
     if (shape.tile_size == 8 && rpl == 2) k_forward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
     else if (shape.tile_size == 8) k_forward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
     else k_forward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
@@ -924,6 +949,7 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     RenderArgs a{};
     fill_shape(a, shape);
     a.recs = cat<Rec>(ws_gauss, G.rec);
+    a.ext = cat<float4>(ws_gauss, G.ext);
     a.ranges = cat<int2>(ws_gauss, G.ranges);
     a.pair_ids = capacity > 0 ? cat<int32_t>(ws_pairs, P.vals_out) : nullptr;
     a.gvol = grad_volume;
@@ -935,7 +961,10 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     } else {
         GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
     }
-    if (tuning) a.chunk = tuning->chunk;
+    if (tuning) {
+        a.chunk = tuning->chunk;
+        a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
+    }
     const int rpl = (tuning && !det) ? tuning->rows_per_lane : 2;  // deterministic: whole tiles
     if (capacity > 0) {
         if (shape.tile_size == 8) {
@@ -1054,6 +1083,7 @@ int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, void* ws_
         RenderArgs a{};
         fill_shape(a, it.shape);
         a.recs = cat<Rec>(it.ws_gauss, G.rec);
+        a.ext = cat<float4>(it.ws_gauss, G.ext);
         a.ranges = cat<int2>(it.ws_gauss, G.ranges);
         a.pair_ids = it.capacity > 0 ? cat<int32_t>(it.ws_pairs, P.vals_out) : nullptr;
         a.vol = it.volume;

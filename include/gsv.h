@@ -50,7 +50,7 @@
 extern "C" {
 #endif
 
-#define GSV_ABI_VERSION 1
+#define GSV_ABI_VERSION 2
 
 typedef enum gsv_status {
     GSV_OK = 0,
@@ -186,11 +186,16 @@ GSV_API int gsv_backward_batched(void* ws_batch, int count, int flags, void* str
 /* No counterpart in the reference.  rows_per_lane: 2 = one CTA per 8^3 tile
  * (two 8-voxel rows per lane), 1 = one CTA per 4x8x8 half tile (one row per
  * lane; the deterministic backward always uses whole tiles).  chunk: number
- * of Gaussians a warp stages in shared memory at a time (1..32).  Tile edge 8
- * only; other tile edges ignore it. */
+ * of Gaussians a warp stages in shared memory at a time (1..32).  flags:
+ * GSV_TUNE_NO_CULL turns off the extent cull (a Gaussian, or a 4x8x8 row
+ * slot of it, whose conservative tight extent misses the CTA's voxels is
+ * skipped; it contributes nothing there either way).  Tile edge 8 only;
+ * other tile edges ignore it. */
+#define GSV_TUNE_NO_CULL 0x1
 typedef struct gsv_tuning {
     int32_t rows_per_lane;
     int32_t chunk;
+    int32_t flags;
 } gsv_tuning;
 
 /* gsv_forward / gsv_backward with an explicit execution shape (NULL =

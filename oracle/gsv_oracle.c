@@ -621,3 +621,92 @@ ORC_EXPORT int64_t orc_boundary_voxels(const float* pos, const float* scl, const
     free(g64);
     return count;
 }
+
+/* Extent cull of the tile-8 render kernels, checked against the shared FP32
+ * predicate.  The kernels skip a Gaussian (or a 4x8x8 row slot of it) whose
+ * conservative tight extent ext_a -- 3 sqrt(S_aa (1 + 1e-4 K)) + 0.01 voxel,
+ * S = Q^-1 and K = max_a Q_aa S_aa, infinite when Q is not positive
+ * definite or K > 1e4, computed in FP64 and rounded up to FP32 -- misses
+ * the slot: c_a - ext_a > hi_a or c_a + ext_a < lo_a, in FP32.  Restated
+ * here from that rule.  For every listed (voxel, Gaussian) pair that the
+ * FP32 predicate includes, the voxel's slot must pass that test; returns the
+ * number of included pairs that would be culled (must be 0) and, in
+ * stats[0..2], the pairs listed, the pairs kept and the row slots kept
+ * (slots: the two 4x8x8 halves of each 8^3 tile). */
+static float ext_f32_up(double v) {
+    float f = (float)v;
+    if ((double)f < v) f = nextafterf(f, INFINITY);
+    return f;
+}
+
+static void extent_of(const float* qc, float ext[3]) {
+    double q00 = qc[0], q01 = 0.5 * (double)qc[1], q02 = 0.5 * (double)qc[2];
+    double q11 = qc[3], q12 = 0.5 * (double)qc[4], q22 = qc[5];
+    double c00 = q11 * q22 - q12 * q12, c11 = q00 * q22 - q02 * q02, c22 = q00 * q11 - q01 * q01;
+    double c01 = q02 * q12 - q01 * q22, c02 = q01 * q12 - q02 * q11;
+    double det = q00 * c00 + q01 * c01 + q02 * c02;
+    ext[0] = ext[1] = ext[2] = INFINITY;
+    if (!(q00 > 0.0 && c22 > 0.0 && det > 0.0 && c00 > 0.0 && c11 > 0.0)) return;
+    double s[3] = {c00 / det, c11 / det, c22 / det};
+    double k = fmax(fmax(q00 * s[0], q11 * s[1]), q22 * s[2]);
+    if (!(k <= 1e4)) return;
+    double f = 9.0 * (1.0 + 1e-4 * k);
+    for (int a = 0; a < 3; ++a) ext[a] = ext_f32_up(sqrt(f * s[a]) + 0.01);
+}
+
+static int slot_live(const float* c, const float* ext, const int32_t lo[3], const int32_t hi[3]) {
+    for (int a = 0; a < 3; ++a) {
+        float l = c[a] - ext[a], u = c[a] + ext[a];
+        if (!(l <= (float)hi[a] && u >= (float)lo[a])) return 0;
+    }
+    return 1;
+}
+
+ORC_EXPORT int64_t orc_extent_check(const float* pos, const float* scl, const float* rot, int64_t n,
+                                    int32_t d, int32_t h, int32_t w, const int32_t* tile_ranges,
+                                    const int32_t* pair_ids, int64_t* stats) {
+    const int32_t ts = 8;
+    shape_t sh = mkshape(d, h, w, ts);
+    int64_t nn = n ? n : 1;
+    float* cen = (float*)malloc((size_t)nn * 3 * sizeof(float));
+    float* qc = (float*)malloc((size_t)nn * 6 * sizeof(float));
+    float* ext = (float*)malloc((size_t)nn * 3 * sizeof(float));
+    orc_preprocess_f32(pos, scl, rot, n, d, h, w, cen, NULL, qc);
+    for (int64_t g = 0; g < n; ++g) extent_of(&qc[g * 6], &ext[g * 3]);
+    int64_t bad = 0, listed = 0, kept = 0, slots = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad, listed, kept, slots)
+    for (int64_t t = 0; t < sh.ntiles; ++t) {
+        int32_t s0 = tile_ranges[t * 2], s1 = tile_ranges[t * 2 + 1];
+        int32_t o[3];
+        tile_origin(&sh, t, o);
+        for (int32_t p = s0; p < s1; ++p) {
+            const int32_t g = pair_ids[p];
+            const float* c = &cen[g * 3];
+            int any = 0;
+            for (int half = 0; half < 2; ++half) {
+                int32_t lo[3] = {o[0] + 4 * half, o[1], o[2]};
+                int32_t hi[3] = {o[0] + 4 * half + 3, o[1] + 7, o[2] + 7};
+                int live = slot_live(c, &ext[g * 3], lo, hi);
+                any |= live;
+                slots += live;
+                for (int32_t i = lo[0]; i <= hi[0] && i < d; ++i)
+                    for (int32_t j = lo[1]; j <= hi[1] && j < h; ++j)
+                        for (int32_t k = lo[2]; k <= hi[2] && k < w; ++k) {
+                            float e0 = (float)i - c[0], e1 = (float)j - c[1], e2 = (float)k - c[2];
+                            if (included_f32(&qc[g * 6], e0, e1, e2) && !live) ++bad;
+                        }
+            }
+            ++listed;
+            kept += any;
+        }
+    }
+    free(cen);
+    free(qc);
+    free(ext);
+    if (stats) {
+        stats[0] = listed;
+        stats[1] = kept;
+        stats[2] = slots;
+    }
+    return bad;
+}

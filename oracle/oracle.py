@@ -75,6 +75,9 @@ def lib():
                                               _i32p, _i32p, ctypes.c_double,
                                               np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")]
             L.orc_boundary_voxels.restype = _i64
+            L.orc_extent_check.argtypes = [_f32p, _f32p, _f32p, _i64, _i32, _i32, _i32, _i32p, _i32p,
+                                           np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
+            L.orc_extent_check.restype = _i64
             L.orc_num_threads.argtypes = []
             L.orc_num_threads.restype = ctypes.c_int
             _lib = L
@@ -244,6 +247,20 @@ def boundary_voxels(positions, scales, rotations, shape, tile_size, tile_ranges,
                               np.asarray(positions).shape[0], d, h, w, tile_size, _c(tile_ranges, np.int32),
                               pid, float(tol), flags)
     return flags.reshape(d, h, w).astype(bool)
+
+
+def extent_check(positions, scales, rotations, shape, tile_ranges, pair_ids):
+    """Checks the tile-8 kernels' extent cull against the shared FP32
+    predicate: returns (included pairs the cull would drop -- must be 0,
+    {"listed", "kept", "slots_kept"} counts)."""
+    d, h, w = shape
+    stats = np.zeros(3, np.int64)
+    pid = _c(pair_ids, np.int32)
+    if pid.size == 0:
+        pid = np.zeros(1, np.int32)
+    bad = lib().orc_extent_check(_c(positions, np.float32), _c(scales, np.float32), _c(rotations, np.float32),
+                                 np.asarray(positions).shape[0], d, h, w, _c(tile_ranges, np.int32), pid, stats)
+    return int(bad), {"listed": int(stats[0]), "kept": int(stats[1]), "slots_kept": int(stats[2])}
 
 
 def num_threads() -> int:

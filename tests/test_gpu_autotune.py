@@ -9,7 +9,7 @@ import pytest
 import torch
 
 from gs_tmi_b200 import autotune, synthetic
-from gs_tmi_b200._lib import GsvGrads, GsvParams, GsvTuning, check, lib
+from gs_tmi_b200._lib import GSV_BACKWARD_DETERMINISTIC, GSV_TUNE_NO_CULL, GsvGrads, GsvParams, GsvTuning, check, lib
 from gs_tmi_b200.tile_voxelizer import _ptr, _shape, prepare_and_bin
 from oracle import oracle as O
 from tests.helpers import FWD_TOL, GRAD_TOL, rel
@@ -69,3 +69,44 @@ def test_tuner_picks_and_caches(tmp_path, cuda_device):
     t2 = again.pick(plan, params)
     assert (t2.rows_per_lane, t2.chunk) == (t1.rows_per_lane, t1.chunk) and not again.timings
     assert json.loads(path.read_text())[k] == [t1.rows_per_lane, t1.chunk]
+
+
+def _aniso_set(n, shape, seed, spread=1.5):
+    rng = np.random.default_rng(seed)
+    pos = torch.tensor(rng.uniform(-1.1, 1.1, (n, 3)), dtype=torch.float32)
+    vox = np.exp(rng.normal(np.log(2.0), spread, (n, 3)))
+    scl = torch.tensor(vox / (np.array(shape) / 2), dtype=torch.float32)
+    q = torch.tensor(rng.normal(size=(n, 4)), dtype=torch.float32)
+    dr = torch.tensor(rng.normal(0, 0.1, n), dtype=torch.float32)
+    di = torch.tensor(rng.normal(0, 0.1, n), dtype=torch.float32)
+    return synthetic.GaussianSet(pos, scl, q, dr, di)
+
+
+@pytest.mark.parametrize("kind", ["random", "aniso", "edge"])
+@pytest.mark.parametrize("rpl", [2, 1])
+def test_extent_cull_changes_nothing(kind, rpl, cuda_device):
+    """Forward volume and deterministic gradients are bitwise equal with the
+    extent cull on and off (a culled Gaussian adds nothing where it is
+    culled); the atomic backward agrees within its own run-to-run spread
+    (atomic order; large for strongly anisotropic sets, whose per-Gaussian
+    sums cancel heavily)."""
+    shape = (40, 48, 32)
+    gs = {"random": lambda: synthetic.random_gaussians(3000, shape, seed=71),
+          "aniso": lambda: _aniso_set(3000, shape, 72),
+          "edge": lambda: synthetic.concat(synthetic.edge_case_gaussians(shape),
+                                           synthetic.random_gaussians(500, shape, seed=73))}[kind]()
+    gv = synthetic.upstream_grad(shape, seed=74).to(cuda_device)
+    params = tuple(t.to(cuda_device) for t in gs.tensors())
+    det = prepare_and_bin(params, _shape(shape, 8), flags=GSV_BACKWARD_DETERMINISTIC)
+    on = _run(det, params, gv, GsvTuning(rpl, 32, 0))
+    off = _run(det, params, gv, GsvTuning(rpl, 32, GSV_TUNE_NO_CULL))
+    assert np.array_equal(on[0], off[0])
+    for a, b in zip(on[1], off[1]):
+        assert np.array_equal(a, b)
+    plan = prepare_and_bin(params, _shape(shape, 8))
+    on = _run(plan, params, gv, GsvTuning(rpl, 16, 0))
+    off = _run(plan, params, gv, GsvTuning(rpl, 16, GSV_TUNE_NO_CULL))
+    off2 = _run(plan, params, gv, GsvTuning(rpl, 16, GSV_TUNE_NO_CULL))
+    assert np.array_equal(on[0], off[0])
+    for a, b, c in zip(on[1], off[1], off2[1]):
+        assert rel(a, b) <= max(10 * rel(c, b), 1e-5)
