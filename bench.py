@@ -53,6 +53,20 @@ OPS_FWD, OPS_BWD = 15, 33
 SMS, LANES = 148, 128
 
 
+def max_over_ranks(values, dist, device):
+    """Per-rank device times -> their maximum over all ranks (replicas are
+    timed by the slowest one)."""
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(units_per_step, steps, world, total_ms):
+    """Units processed by all replicas per second, timed by the slowest rank."""
+    return units_per_step * steps * world / (total_ms * 1e-3)
+
+
 def make_inputs(name):
     from gs_tmi_b200 import synthetic
 
@@ -144,13 +158,10 @@ def run_batched(args, rank, world, dist):
         torch.cuda.synchronize(dev)
     lat = sorted(a.elapsed_time(b) for a, b in ev)
     total_ms = sum(lat)
-    stats = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
-    total_ms = float(stats[0])
+    total_ms, = max_over_ranks([total_ms], dist, dev)
     if rank != 0:
         return
-    out = {"metric": "fwd+bwd Gvox-evals/s", "value": evals * args.steps * world / (total_ms * 1e-3) / 1e9,
+    out = {"metric": "fwd+bwd Gvox-evals/s", "value": whole_job_rate(evals, args.steps, world, total_ms) / 1e9,
            "unit": "Gvox-evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "fp32", "data": "synthetic",
@@ -443,10 +454,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.synchronize(dev)
     e2e_ms = e0.elapsed_time(e1)
 
-    stats = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = stats.tolist()
+    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
     if rank != 0:
         return
     pk, pk_kind = peaks()
@@ -462,7 +470,7 @@ def run_ours(args, rank, world, dist):
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(name, {}).get("k_backward8")
     vol_bytes = 2 * 8 * d * h * w  # write the volume, read its gradient
-    value = evals * args.steps * world / (total_ms * 1e-3) / 1e9
+    value = whole_job_rate(evals, args.steps, world, total_ms) / 1e9
     out = {
         "metric": "fwd+bwd Gvox-evals/s", "value": value, "unit": "Gvox-evals/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -481,7 +489,7 @@ def run_ours(args, rank, world, dist):
                      "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
                      "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9,
                              "peak_gbs": pk.get("hbm_gbs")}},
-        "e2e": {"value": evals * args.steps * world / (e2e_ms * 1e-3) / 1e9, "unit": "Gvox-evals/s",
+        "e2e": {"value": whole_job_rate(evals, args.steps, world, e2e_ms) / 1e9, "unit": "Gvox-evals/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
                 "api": "gs_tmi_b200.TileVoxelizer forward + autograd backward"},
         "gpu_launches": None if n_launch is None else n_launch * args.steps,

@@ -83,7 +83,7 @@ SIGNATURES = {
     "gsv_build_tile_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _vp, _i64, _i64p, _vp]),
     "gsv_mlp_gemm": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
                                     ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
-                                    _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _vp, _vp]),
+                                    _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _vp, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),
 }

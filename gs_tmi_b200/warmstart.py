@@ -46,13 +46,13 @@ def _p(t: Optional[torch.Tensor]):
 
 
 def gemm(a, a_strides, b, b_strides, M, N, K, epi, out_f32=None, out_bf16=None, z=None, bias=None,
-         c_strides=None, splits=1, err=None):
+         c_strides=None, splits=1, err=None, col_sum=None):
     """C = A B^T on the tcgen05 kernel (see include/gsv.h, gsv_mlp_gemm)."""
     if err is None:
         err = torch.zeros(1, dtype=torch.int32, device=a.device)
     c_sm, c_sn = c_strides if c_strides else (N, 1)
     check(lib.gsv_mlp_gemm(_p(a), a_strides[0], a_strides[1], _p(b), b_strides[0], b_strides[1], M, N, K, splits,
-                           _p(bias), _p(out_f32), _p(out_bf16), _p(z), c_sm, c_sn, epi, _p(err),
+                           _p(bias), _p(out_f32), _p(out_bf16), _p(z), c_sm, c_sn, epi, _p(col_sum), _p(err),
                            ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)), "gsv_mlp_gemm")
     return err
 
@@ -164,14 +164,18 @@ class WarmStartMLP:
         gemm(y2, (1, HID), dob, (1, OUT), HID, OUT, B, EPI_ATOMIC_F32, out_f32=dW3, c_strides=(1, HID),
              splits=splits, err=self.err)
         dz2 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
-        gemm(dob, (OUT, 1), self.wb[2], (1, HID), B, HID, OUT, EPI_GELU_GRAD, out_bf16=dz2, z=z2, err=self.err)
+        db2 = torch.zeros(HID, device=dev)
+        gemm(dob, (OUT, 1), self.wb[2], (1, HID), B, HID, OUT, EPI_GELU_GRAD, out_bf16=dz2, z=z2, err=self.err,
+             col_sum=db2)
         dW2 = torch.zeros(HID, HID, device=dev)
         gemm(dz2, (1, HID), y1, (1, HID), HID, HID, B, EPI_ATOMIC_F32, out_f32=dW2, splits=splits, err=self.err)
         dz1 = torch.empty(B, HID, device=dev, dtype=torch.bfloat16)
-        gemm(dz2, (HID, 1), self.wb[1], (1, HID), B, HID, HID, EPI_GELU_GRAD, out_bf16=dz1, z=z1, err=self.err)
+        db1 = torch.zeros(HID, device=dev)
+        gemm(dz2, (HID, 1), self.wb[1], (1, HID), B, HID, HID, EPI_GELU_GRAD, out_bf16=dz1, z=z1, err=self.err,
+             col_sum=db1)
         dW1 = torch.zeros(HID, IN, device=dev)
         gemm(dz1, (1, HID), x, (1, IN), HID, IN, B, EPI_ATOMIC_F32, out_f32=dW1, splits=splits, err=self.err)
-        return [dW1, dW2, dW3, dz1.float().sum(0), dz2.float().sum(0), dout.sum(0)]
+        return [dW1, dW2, dW3, db1, db2, dout.sum(0)]
 
     def check_ok(self):
         if int(self.err.item()) != 0:
@@ -294,3 +298,46 @@ def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed:
     pos, scl, rot, dr, di = decode(out, vox, base, tuple(case.ground_truth.shape), scale)
     return synthetic.GaussianSet(pos.contiguous(), scl.contiguous(), rot.contiguous(), dr.contiguous(),
                                  di.contiguous())
+
+
+def time_training_pass(batch: int = 65536, iters: int = 5, device="cuda:0", seed: int = 0) -> dict:
+    """CUDA-event time of one MLP forward + backward (8 tcgen05 GEMMs) on a
+    random BF16 batch, with the bytes those GEMMs must move at least: every
+    operand read once, every output written once."""
+    mlp = WarmStartMLP(device, seed=seed)
+    g = torch.Generator(device=device).manual_seed(seed)
+    x = torch.randn(batch, IN, device=device, generator=g).bfloat16()
+    dout = torch.randn(batch, OUT, device=device, generator=g) / batch
+    for _ in range(2):
+        mlp.backward(mlp.forward(x)[1], dout)
+    torch.cuda.synchronize(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(iters):
+        mlp.backward(mlp.forward(x)[1], dout)
+    e1.record()
+    torch.cuda.synchronize(device)
+    mlp.check_ok()
+    ms = e0.elapsed_time(e1) / iters
+    b = batch
+    # forward: x, y1, y2 read (bf16); z1, z2 (f32) + y1, y2 (bf16) + out (f32) written
+    fwd = 2 * b * (IN + 2 * HID) + b * (4 + 2) * 2 * HID + 4 * b * OUT
+    bwd = (2 * b * (HID + OUT)                        # dW3: y2, dout
+           + 2 * b * OUT + 4 * b * HID + 2 * b * HID  # dz2: dout, z2 -> dz2
+           + 4 * b * HID                              # dW2: dz2, y1
+           + 2 * b * HID + 4 * b * HID + 2 * b * HID  # dz1: dz2, z1 -> dz1
+           + 2 * b * (HID + IN))                      # dW1: dz1, x
+    flops = 2 * b * (IN * HID + HID * HID + HID * OUT) * 3
+    return {"batch": batch, "ms": ms, "min_bytes": fwd + bwd, "gbs": (fwd + bwd) / (ms * 1e-3) / 1e9,
+            "tflops": flops / (ms * 1e-3) / 1e12}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="time one warm-start MLP training pass on the tcgen05 GEMMs")
+    ap.add_argument("--batch", type=int, default=65536)
+    ap.add_argument("--iters", type=int, default=5)
+    a = ap.parse_args()
+    print(json.dumps(time_training_pass(a.batch, a.iters)))

@@ -248,12 +248,14 @@ GSV_API int gsv_build_tile_pairs_noalloc(const float* center_vox, const float* r
  * epi: 0 = FP32 store of acc (+ bias[n] if bias), 1 = z_f32 = acc + bias,
  * out_bf16 = GELU(z), 2 = out_bf16 = acc * GELU'(z_f32), 3 = atomicAdd of
  * acc into out_f32 (required when splits > 1: K split across CTAs).
- * N must be a multiple of 16.  *error (device int) becomes 1 if a wait on
- * the tensor cores timed out. */
+ * col_sum (optional, epi 2 with c_sn == 1 only): col_sum[n] += sum over m of
+ * the BF16 output (the bias gradient of the layer), accumulated with
+ * atomics; zero it first.  N must be a multiple of 16.  *error (device int)
+ * becomes 1 if a wait on the tensor cores timed out. */
 GSV_API int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, long long b_sn,
                          long long b_sk, int M, int N, int K, int splits, const float* bias, float* out_f32,
-                         void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, int* error,
-                         void* stream);
+                         void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, float* col_sum,
+                         int* error, void* stream);
 
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 

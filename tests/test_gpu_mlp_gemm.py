@@ -21,11 +21,11 @@ def _p(t):
 
 
 def gemm(a, a_strides, b, b_strides, M, N, K, epi, out_f32=None, out_bf16=None, z=None, bias=None, c_strides=None,
-         splits=1):
+         splits=1, col_sum=None):
     err = torch.zeros(1, dtype=torch.int32, device=a.device)
     c_sm, c_sn = c_strides if c_strides else (N, 1)
     check(lib.gsv_mlp_gemm(_p(a), a_strides[0], a_strides[1], _p(b), b_strides[0], b_strides[1], M, N, K, splits,
-                           _p(bias), _p(out_f32), _p(out_bf16), _p(z), c_sm, c_sn, epi, _p(err),
+                           _p(bias), _p(out_f32), _p(out_bf16), _p(z), c_sm, c_sn, epi, _p(col_sum), _p(err),
                            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "gsv_mlp_gemm")
     torch.cuda.synchronize()
     assert int(err.item()) == 0, "tensor-core wait timed out"
@@ -48,9 +48,11 @@ def test_gemm_f32_k_major(M, N, K, cuda_device):
     assert rel(out, ref) < 1e-5
 
 
-def test_gemm_transposed_operands_split_k(cuda_device):
-    """Weight-gradient shape: C = dZ^T X with K = batch, split over CTAs."""
-    B, F1, F2 = 4096, 256, 256
+@pytest.mark.parametrize("B,F1,F2", [(4096, 256, 256), (1000, 240, 196), (777, 16, 256)])
+def test_gemm_transposed_operands_split_k(B, F1, F2, cuda_device):
+    """Weight-gradient shape: C = dZ^T X with K = batch, split over CTAs
+    (row-contiguous operands: MN-major copies; F2 = 196 takes the
+    element-wise path for A)."""
     g = torch.Generator(device=cuda_device).manual_seed(3)
     dz = torch.randn(B, F2, device=cuda_device, generator=g).bfloat16()
     x = torch.randn(B, F1, device=cuda_device, generator=g).bfloat16()
@@ -81,7 +83,10 @@ def test_gemm_gelu_epilogues(cuda_device):
     dy = torch.randn(M, N, device=cuda_device, generator=g).bfloat16()
     dz = torch.empty(M, K, device=cuda_device, dtype=torch.bfloat16)
     zin = torch.randn(M, K, device=cuda_device, generator=g)
-    gemm(dy, (N, 1), w, (1, K), M, K, N, EPI_GELU_GRAD, out_bf16=dz, z=zin)
+    colsum = torch.zeros(K, device=cuda_device)
+    gemm(dy, (N, 1), w, (1, K), M, K, N, EPI_GELU_GRAD, out_bf16=dz, z=zin, col_sum=colsum)
     zz = zin.clone().requires_grad_(True)
     torch.nn.functional.gelu(zz).backward(dy.float() @ w.float())
     assert rel(dz.float(), zz.grad) < 1e-2
+    # fused bias gradient: column sums of the stored BF16 output
+    assert rel(colsum, dz.float().sum(0)) < 1e-5
