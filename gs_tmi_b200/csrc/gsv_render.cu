@@ -213,10 +213,11 @@ static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 
 // Stages Gaussians [base, base + cnt) of the tile list and returns how many
 // were kept.  Native layout: a Gaussian is kept only if its conservative
-// tight extent (Rec + ext, see tight_extent) reaches the CTA's rows, and it
-// carries one bit per row slot it reaches; a dropped Gaussian or slot has
-// m > 9 at every voxel there, so skipping it changes no sum.  The kept
-// Gaussians keep their list order.  Compat layout: everything is kept.
+// tight extent (see tight_extent) reaches the CTA's rows, and it carries
+// one bit per row slot it reaches; a dropped Gaussian or slot has m > 9 at
+// every voxel there, so skipping it changes no sum.  The kept Gaussians keep
+// their list order.  The native layout reads the extent k_prepare stored,
+// the compat layout (cov_inv input) computes it here.
 template <bool COMPAT, int RPL>
 __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int d0,
                                            int h0, int w0, int sub, const float ih[3]) {
@@ -225,10 +226,18 @@ __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, in
     if (lane < cnt) {
         gid = __ldg(a.pair_ids + base + lane);
         r = load_rec<COMPAT>(a, gid, ih);
-        if (COMPAT || !a.cull) {
+        if (!a.cull) {
             bits = (1 << RPL) - 1;
         } else {
-            const float4 x = __ldg(a.ext + gid);
+            // native layout: precomputed by k_prepare; compat: from the
+            // coefficients just derived from cov_inv (same rule)
+            float4 x;
+            if (COMPAT) {
+                const float qc[6] = {r.q00, r.q01x2, r.q02x2, r.q11, r.q12x2, r.q22};
+                x = tight_extent(qc);
+            } else {
+                x = __ldg(a.ext + gid);
+            }
             const bool hw = __fsub_rn(r.c1, x.y) <= float(h0 + 7) && __fadd_rn(r.c1, x.y) >= float(h0) &&
                             __fsub_rn(r.c2, x.z) <= float(w0 + 7) && __fadd_rn(r.c2, x.z) >= float(w0);
             const float lo = __fsub_rn(r.c0, x.x), hi = __fadd_rn(r.c0, x.x);
@@ -509,7 +518,10 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
 }
 
 template <bool COMPAT, bool DET, int RPL>
-__global__ void __launch_bounds__(kThreads) k_backward8(const RenderArgs a) {
+// Register cap: 6 resident CTAs per SM for whole tiles (80 registers), 7 for
+// half tiles (72); a few spilled bytes outside the inner loop cost less
+// than the occupancy they buy (measured on B200).
+__global__ void __launch_bounds__(kThreads, RPL == 2 ? 6 : 7) k_backward8(const RenderArgs a) {
     __shared__ __align__(16) WarpStage stage[kWarps];
     constexpr int subs = 2 / RPL;
     backward_tile<COMPAT, DET, RPL>(a, blockIdx.x / subs, blockIdx.x % subs, stage);
@@ -809,7 +821,7 @@ __global__ void __launch_bounds__(kThreads) k_forward8_batched(const BatchTable 
 }
 
 template <bool DET>
-__global__ void __launch_bounds__(kThreads) k_backward8_batched(const BatchTable t) {
+__global__ void __launch_bounds__(kThreads, 6) k_backward8_batched(const BatchTable t) {
     __shared__ __align__(16) WarpStage stage[kWarps];
     __shared__ long long s_next;
     const int64_t total = t.tile_prefix[t.count];
@@ -1136,10 +1148,13 @@ BatchTable batch_table(void* ws_batch, int count, int det) {
     return t;
 }
 
-int persistent_grid() {
-    int dev = 0, sms = 148;
+// Persistent grid: every SM filled to the kernel's occupancy.
+int persistent_grid(const void* kernel, int threads) {
+    int dev = 0, sms = 148, per_sm = 4;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms * 4;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 4;
+    return sms * per_sm;
 }
 }  // namespace
 
@@ -1148,7 +1163,7 @@ int gsv_forward_batched(void* ws_batch, int count, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     BatchTable t = batch_table(ws_batch, count, 0);
     GSV_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 2 * sizeof(unsigned long long), st));
-    k_forward8_batched<<<persistent_grid(), kThreads, 0, st>>>(t);
+    k_forward8_batched<<<persistent_grid(reinterpret_cast<const void*>(k_forward8_batched), kThreads), kThreads, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }
@@ -1159,11 +1174,11 @@ int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream) {
     const bool det = flags & GSV_BACKWARD_DETERMINISTIC;
     BatchTable t = batch_table(ws_batch, count, det);
     GSV_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 2 * sizeof(unsigned long long), st));
-    const int grid = persistent_grid();
+    const int grid = persistent_grid(reinterpret_cast<const void*>(k_zero_batched), 256);
     k_zero_batched<<<grid, 256, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
-    if (det) k_backward8_batched<true><<<grid, kThreads, 0, st>>>(t);
-    else k_backward8_batched<false><<<grid, kThreads, 0, st>>>(t);
+    if (det) k_backward8_batched<true><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<true>), kThreads), kThreads, 0, st>>>(t);
+    else k_backward8_batched<false><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<false>), kThreads), kThreads, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
     if (det) k_finalize_batched<true><<<grid, 256, 0, st>>>(t);
     else k_finalize_batched<false><<<grid, 256, 0, st>>>(t);
