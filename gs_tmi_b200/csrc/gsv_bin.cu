@@ -220,38 +220,53 @@ __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ 
 }
 
 // One thread per Gaussian writes its (tile, gid) pairs in raster order.
+// One warp per 32 consecutive Gaussians.  Their pairs occupy one contiguous
+// range of the output (offsets is an exclusive scan), which the lanes cover
+// side by side: lane l writes pairs start+l, start+l+32, ... and finds the
+// Gaussian a pair belongs to by a 5-step search over the warp's 32 offsets
+// (coalesced, balanced however the pair counts are spread).  Tiles follow
+// the (d,h,w) raster order of each Gaussian's tile box.
 __global__ void __launch_bounds__(128) k_emit(const int4* __restrict__ boxes,
                                               const int64_t* __restrict__ offsets, int64_t n,
                                               DevShape s, int64_t cap, int32_t* __restrict__ keys,
                                               int32_t* __restrict__ vals, Status* status) {
+    constexpr unsigned kAll = 0xffffffffu;
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     if (g == 0) {
         const int64_t total = offsets[n];
         if (total > cap) atomicOr(&status->flags, GSV_FLAG_CAPACITY_OVERFLOW);
         if (total > int64_t(INT32_MAX)) atomicOr(&status->flags, GSV_FLAG_TOO_MANY_PAIRS);
     }
-    if (g >= n) return;
-    const int4 b = boxes[g];
-    const int32_t cnt = b.w;
-    if (cnt <= 0) return;
-    const int32_t t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
-    const int32_t n0 = (b.y >> 16) & 0xffff, n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
-    (void)n0;
-    int64_t o = offsets[g];
-    const int32_t gid = int32_t(g);
-    for (int32_t i = 0, j = 0, k = 0, c = 0; c < cnt; ++c) {
-        if (o >= cap) break;
-        const int32_t tile = ((t0 + i) * s.nt[1] + (t1 + j)) * s.nt[2] + (t2 + k);
-        keys[o] = tile;
-        vals[o] = gid;
-        ++o;
-        if (++k == n2) {
-            k = 0;
-            if (++j == n1) {
-                j = 0;
-                ++i;
-            }
+    const int64_t g0 = g - lane;  // first Gaussian of this warp (warp-uniform)
+    if (g0 >= n) return;
+    const int m = int(min(int64_t(32), n - g0));
+    const long long end = offsets[g0 + m];  // one past the warp's last pair
+    int4 b = make_int4(0, 0, 0, 0);
+    long long o = end;                      // lanes past the last Gaussian never match
+    if (lane < m) {
+        b = boxes[g];
+        o = offsets[g];
+    }
+    const long long start = __shfl_sync(kAll, o, 0);
+    for (long long base = start; base < end; base += 32) {
+        const long long p = base + lane;
+        int j = 0;  // largest j with o_j <= p
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            const long long oj = __shfl_sync(kAll, o, j + step);
+            if (oj <= p) j += step;
         }
+        const long long oj = __shfl_sync(kAll, o, j);
+        const int bx = __shfl_sync(kAll, b.x, j), by = __shfl_sync(kAll, b.y, j), bz = __shfl_sync(kAll, b.z, j);
+        if (p >= end || p >= cap) continue;
+        const int32_t c = int32_t(p - oj);
+        const int32_t t0 = bx & 0xffff, t1 = (bx >> 16) & 0xffff, t2 = by & 0xffff;
+        const int32_t n1 = bz & 0xffff, n2 = (bz >> 16) & 0xffff;
+        const int32_t k = c % n2, r = c / n2;
+        const int32_t jj = r % n1, i = r / n1;
+        keys[p] = ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
+        vals[p] = int32_t(g0 + j);
     }
 }
 

@@ -3,8 +3,10 @@
 // Work decomposition (tile edge 8, the reference default):
 //   one CTA of 4 warps per tile; every warp covers the whole 8x8x8 tile
 //   (lane l owns the two 8-voxel rows (d0+l/8, h0+l%8) and (d0+4+l/8, h0+l%8))
-//   and the tile's Gaussian list is split between the warps in chunks of 32.
-//   A warp stages its 32 Gaussians in shared memory, then walks them; for
+//   and the tile's Gaussian list is dealt out to the warps position by
+//   position (warp w takes positions w, w+4, ...).  A warp stages up to 32
+//   of its Gaussians in shared memory, drops those whose tight extent
+//   misses the CTA's voxels, then walks the rest; for
 //   each Gaussian a lane evaluates its 16 voxels with the row form
 //   m = fma(fma(q22, e2, B), e2, A) (A, B once per row), and the exp / FMA
 //   part runs only when some lane of the warp is inside the 3-sigma cutoff.
@@ -200,19 +202,21 @@ struct __align__(16) WarpStage {
     Rec rec[32];
     float4 e2[32][2];
     int32_t gid[32];
-    int32_t meta[32];  // bit r: row slot r may hold included voxels; bits 8+: position in the chunk
+    int32_t meta[32];  // bit r: row slot r may hold included voxels; bits 8+: index in the chunk
 };
 
 // Execution shape of a CTA on an 8^3 binning tile.  RPL (rows per lane) = 2:
 // the CTA covers the whole tile, lane l owns rows (d0+l/8, h0+l%8) and
 // (d0+4+l/8, h0+l%8).  RPL = 1: the CTA covers the 4x8x8 half `sub` of the
 // tile, lane l owns row (d0+4*sub+l/8, h0+l%8).  Either way each warp walks
-// its share of the tile's Gaussian list in chunks of `a.chunk` (<= 32).
+// its share of the tile's Gaussian list (every 4th position) in chunks of
+// `a.chunk` (<= 32).
 constexpr int kFwdSmem = kWarps * 16 * 32 * sizeof(float2);
 static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 
-// Stages Gaussians [base, base + cnt) of the tile list and returns how many
-// were kept.  Native layout: a Gaussian is kept only if its conservative
+// Stages list positions base, base + kWarps, ..., (cnt of them: warp w of
+// a CTA walks positions w, w + 4, w + 8, ... so the warps' shares differ by
+// at most one Gaussian) and returns how many were kept.  Native layout: a Gaussian is kept only if its conservative
 // tight extent (see tight_extent) reaches the CTA's rows, and it carries
 // one bit per row slot it reaches; a dropped Gaussian or slot has m > 9 at
 // every voxel there, so skipping it changes no sum.  The kept Gaussians keep
@@ -224,7 +228,7 @@ __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, in
     Rec r;
     int gid = 0, bits = 0;
     if (lane < cnt) {
-        gid = __ldg(a.pair_ids + base + lane);
+        gid = __ldg(a.pair_ids + base + kWarps * lane);
         r = load_rec<COMPAT>(a, gid, ih);
         if (!a.cull) {
             bits = (1 << RPL) - 1;
@@ -287,8 +291,10 @@ __device__ __forceinline__ void forward_tile(const RenderArgs& a, int64_t tile, 
         for (int r = 0; r < RPL; ++r) ev0[r] = float(d0 + (lane >> 3) + 4 * (r + sub));
         const float ev1 = float(h0 + (lane & 7));
         WarpStage& S = stage[warp];
-        for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
-            const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, rg.y - base), lane, d0, h0, w0, sub, ih);
+        const int mine = (rg.y - rg.x - warp + kWarps - 1) / kWarps;  // list positions of this warp
+        for (int i0 = 0; i0 < mine; i0 += chunk) {
+            const int base = rg.x + warp + kWarps * i0;
+            const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
             __syncwarp();
             for (int j = 0; j < kept; ++j) {
                 const Rec g = S.rec[j];
@@ -433,8 +439,10 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
     for (int r = 0; r < RPL; ++r) ev0[r] = float(d0 + (lane >> 3) + 4 * (r + sub));
     const float ev1 = float(h0 + (lane & 7));
     WarpStage& S = stage[warp];
-    for (int base = rg.x + warp * chunk; base < rg.y; base += kWarps * chunk) {
-        const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, rg.y - base), lane, d0, h0, w0, sub, ih);
+    const int mine = (rg.y - rg.x - warp + kWarps - 1) / kWarps;  // list positions of this warp
+    for (int i0 = 0; i0 < mine; i0 += chunk) {
+        const int base = rg.x + warp + kWarps * i0;
+        const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
         __syncwarp();
         for (int j = 0; j < kept; ++j) {
             const Rec g = S.rec[j];
@@ -507,7 +515,7 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                 compat_emit(a, g, gid, tot, lane, ih);
             } else if (DET) {
                 if (!(lane & 1) && (lane >> 1) < kMom)
-                    a.partials[int64_t(base + (bits >> 8)) * kMomStride + (lane >> 1)] = tot;
+                    a.partials[int64_t(base + kWarps * (bits >> 8)) * kMomStride + (lane >> 1)] = tot;
             } else {
                 if (!(lane & 1) && (lane >> 1) < kMom)
                     atomicAdd(a.accum + int64_t(gid) * kMomStride + (lane >> 1), tot);
