@@ -45,6 +45,8 @@ WORKLOADS = {
     "batch12": dict(shape=None, n=sum(n for _, n in BATCH12), kind="batch"),
     "mri128x128x96_n500k": dict(shape=(128, 128, 96), n=500_000, kind="from_image"),
     "cube64_n20k": dict(shape=(64, 64, 64), n=20_000, kind="random"),
+    # the large reconstruction at its 2M-Gaussian cap (run with --deterministic)
+    "mri256x256x160_n2m": dict(shape=(256, 256, 160), n=2_000_000, kind="phantom"),
 }
 TILE = 8
 # Algorithmic FP32-pipe operations per candidate evaluation (forward 15,
@@ -74,6 +76,8 @@ def make_inputs(name):
     if wl["kind"] == "from_image":
         case = synthetic.mri_case(wl["shape"], n_coils=8, accel=6.0, calib=24, seed=0)
         gs = synthetic.from_image_init(case.zero_filled, wl["n"], seed=0)
+    elif wl["kind"] == "phantom":  # intensity-seeded on the phantom itself (no coil simulation)
+        gs = synthetic.from_image_init(synthetic.ellipsoid_phantom(wl["shape"], seed=0), wl["n"], seed=0)
     else:
         gs = synthetic.random_gaussians(wl["n"], wl["shape"], seed=0)
     return gs, synthetic.upstream_grad(wl["shape"], seed=1)
