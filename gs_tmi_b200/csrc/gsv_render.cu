@@ -63,7 +63,9 @@ struct RenderArgs {
     const float* gv_r;  // planar
     const float* gv_i;
     float* accum;     // [n, 12] moments (native, atomics)
-    float* partials;  // [pairs, 12] moments (native, deterministic)
+    float* partials;  // [pairs, 12] moments (native, deterministic), at each pair's emission index
+    const int64_t* offsets;  // per-Gaussian first emission index (binning scan)
+    int64_t capacity;        // pair capacity (bound of every emission index)
     float* g_center;  // compat outputs
     float* g_cov;
     float* g_dr;
@@ -203,7 +205,19 @@ struct __align__(16) WarpStage {
     float4 e2[32][2];
     int32_t gid[32];
     int32_t meta[32];  // bit r: row slot r may hold included voxels; bits 8+: index in the chunk
+    int32_t pidx[32];  // deterministic backward: emission index of the (tile, Gaussian) pair
 };
+
+// Emission index of the pair (Gaussian gid, tile (td, th, tw)): the
+// Gaussian's first index plus the tile's raster position in its tile box --
+// where binning emitted it.  Per-pair partials stored at this index lie
+// contiguously per Gaussian, in tile raster order.
+__device__ __forceinline__ int64_t emission_index(const RenderArgs& a, int gid, int td, int th, int tw) {
+    const int4 b = __ldg(a.boxes + gid);
+    const int t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
+    const int n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
+    return __ldg(a.offsets + gid) + (int64_t(td - t0) * n1 + (th - t1)) * n2 + (tw - t2);
+}
 
 // Execution shape of a CTA on an 8^3 binning tile.  RPL (rows per lane) = 2:
 // the CTA covers the whole tile, lane l owns rows (d0+l/8, h0+l%8) and
@@ -222,7 +236,7 @@ static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 // every voxel there, so skipping it changes no sum.  The kept Gaussians keep
 // their list order.  The native layout reads the extent k_prepare stored,
 // the compat layout (cov_inv input) computes it here.
-template <bool COMPAT, int RPL>
+template <bool COMPAT, int RPL, bool DET = false>
 __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int d0,
                                            int h0, int w0, int sub, const float ih[3]) {
     Rec r;
@@ -258,6 +272,7 @@ __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, in
         S.rec[pos] = r;
         S.gid[pos] = gid;
         S.meta[pos] = bits | (lane << 8);
+        if (DET) S.pidx[pos] = int32_t(emission_index(a, gid, d0 >> 3, h0 >> 3, w0 >> 3));
         float e2[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) e2[k] = __fsub_rn(float(w0 + k), r.c2);
@@ -442,7 +457,8 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
     const int mine = (rg.y - rg.x - warp + kWarps - 1) / kWarps;  // list positions of this warp
     for (int i0 = 0; i0 < mine; i0 += chunk) {
         const int base = rg.x + warp + kWarps * i0;
-        const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
+        const int kept =
+            stage_chunk<COMPAT, RPL, DET>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
         __syncwarp();
         for (int j = 0; j < kept; ++j) {
             const Rec g = S.rec[j];
@@ -515,7 +531,7 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                 compat_emit(a, g, gid, tot, lane, ih);
             } else if (DET) {
                 if (!(lane & 1) && (lane >> 1) < kMom)
-                    a.partials[int64_t(base + kWarps * (bits >> 8)) * kMomStride + (lane >> 1)] = tot;
+                    a.partials[int64_t(S.pidx[j]) * kMomStride + (lane >> 1)] = tot;
             } else {
                 if (!(lane & 1) && (lane >> 1) < kMom)
                     atomicAdd(a.accum + int64_t(gid) * kMomStride + (lane >> 1), tot);
@@ -589,6 +605,7 @@ template <bool COMPAT, bool DET>
 __global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs a) {
     __shared__ Rec srec[32];
     __shared__ int sgid[32];
+    __shared__ int64_t sidx[32];
     __shared__ float sred[kWarps][kMom];
     const int64_t tile = blockIdx.x;
     const int2 rg = a.ranges[tile];
@@ -607,6 +624,7 @@ __global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs 
             const int gid = __ldg(a.pair_ids + base + threadIdx.x);
             sgid[threadIdx.x] = gid;
             srec[threadIdx.x] = load_rec<COMPAT>(a, gid, ih);
+            if (DET) sidx[threadIdx.x] = emission_index(a, gid, d0 / ts, h0 / ts, w0 / ts);
         }
         __syncthreads();
         for (int j = 0; j < cnt; ++j) {
@@ -659,7 +677,7 @@ __global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs 
                 if (COMPAT) {
                     compat_emit(a, g, gid, spread, lane, ih);
                 } else if (DET) {
-                    if (lane < kMom) a.partials[int64_t(base + j) * kMomStride + lane] = t;
+                    if (lane < kMom) a.partials[sidx[j] * kMomStride + lane] = t;
                 } else {
                     if (lane < kMom) atomicAdd(a.accum + int64_t(gid) * kMomStride + lane, t);
                 }
@@ -675,41 +693,46 @@ __global__ void __launch_bounds__(kThreads) k_backward_generic(const RenderArgs 
 // tail of the reference), in FP32.
 // ---------------------------------------------------------------------------
 
-template <bool DET>
+// Deterministic moments of Gaussian g, one warp: the Gaussian's per-pair
+// partials sit contiguously at its emission indices, in tile raster order;
+// lane l sums entries l, l + 32, ... and a fixed xor tree sums the lanes.
+// The order depends only on the tile box, so the result is bitwise
+// reproducible.  Writes the moments where the atomic backward accumulates
+// them.
+__device__ __forceinline__ void gather_det_warp(const RenderArgs& a, int64_t g, int lane) {
+    float mo[kMom];
+#pragma unroll
+    for (int i = 0; i < kMom; ++i) mo[i] = 0.f;
+    const int cnt = a.boxes[g].w;
+    const int64_t first = a.offsets[g];
+    for (int c = lane; c < cnt; c += 32) {
+        const int64_t e = first + c;
+        if (e >= a.capacity) break;  // pair capacity overflow (flagged): no such partial
+        const float4* src = reinterpret_cast<const float4*>(a.partials + e * kMomStride);
+        const float4 x = src[0], y = src[1], z = src[2];
+        mo[0] += x.x; mo[1] += x.y; mo[2] += x.z; mo[3] += x.w;
+        mo[4] += y.x; mo[5] += y.y; mo[6] += y.z; mo[7] += y.w;
+        mo[8] += z.x; mo[9] += z.y; mo[10] += z.z;
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+        for (int i = 0; i < kMom; ++i) mo[i] += __shfl_xor_sync(0xffffffffu, mo[i], off);
+    if (lane == 0) {
+        float4* dst = reinterpret_cast<float4*>(a.accum + g * kMomStride);
+        dst[0] = make_float4(mo[0], mo[1], mo[2], mo[3]);
+        dst[1] = make_float4(mo[4], mo[5], mo[6], mo[7]);
+        dst[2] = make_float4(mo[8], mo[9], mo[10], 0.f);
+    }
+}
+
+// Chain rule of one Gaussian from its 11 moments (accum).
 __device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
     const gsv_params& p = a.prm;
     const gsv_grads& out = a.grd;
-    const int4* __restrict__ boxes = a.boxes;
     float mo[kMom];
-    if (!DET) {
 #pragma unroll
-        for (int i = 0; i < kMom; ++i) mo[i] = a.accum[g * kMomStride + i];
-    } else {
-#pragma unroll
-        for (int i = 0; i < kMom; ++i) mo[i] = 0.f;
-        const int4 b = boxes[g];
-        const int t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
-        const int n0 = (b.y >> 16) & 0xffff, n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
-        if (b.w > 0) {
-            for (int i = 0; i < n0; ++i)
-                for (int j = 0; j < n1; ++j)
-                    for (int k = 0; k < n2; ++k) {
-                        const int64_t t = (int64_t(t0 + i) * a.nth + (t1 + j)) * a.ntw + (t2 + k);
-                        const int2 rg = a.ranges[t];
-                        int lo = rg.x, hi = rg.y;  // pair_ids ascending within the tile
-                        while (lo < hi) {
-                            const int mid = (lo + hi) >> 1;
-                            if (a.pair_ids[mid] < int(g)) lo = mid + 1;
-                            else hi = mid;
-                        }
-                        if (lo < rg.y && a.pair_ids[lo] == int(g)) {
-                            const float* src = a.partials + int64_t(lo) * kMomStride;
-#pragma unroll
-                            for (int q = 0; q < kMom; ++q) mo[q] += src[q];
-                        }
-                    }
-        }
-    }
+    for (int i = 0; i < kMom; ++i) mo[i] = a.accum[g * kMomStride + i];
     const Rec R = a.recs[g];
     // dL/dcenter_vox, then dcenter/dpositions = 0.5 * shape = hs   (:284)
     const float dc0 = -(2.0f * R.q00 * mo[2] + R.q01x2 * mo[3] + R.q02x2 * mo[4]);
@@ -779,11 +802,17 @@ __device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
     for (int k = 0; k < 4; ++k) out.rotations[g * 4 + k] = gn[k] / den - q[k] * corr;
 }
 
-template <bool DET>
 __global__ void __launch_bounds__(256) k_finalize(const RenderArgs a) {
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= a.prm.n) return;
-    finalize_one<DET>(a, g);
+    finalize_one(a, g);
+}
+
+// One warp per Gaussian (deterministic backward).
+__global__ void __launch_bounds__(256) k_gather_det(const RenderArgs a) {
+    const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (g >= a.prm.n) return;  // warp-uniform
+    gather_det_warp(a, g, threadIdx.x & 31);
 }
 
 // ---------------------------------------------------------------------------
@@ -858,13 +887,22 @@ __global__ void k_zero_batched(const BatchTable t) {
     }
 }
 
-template <bool DET>
 __global__ void __launch_bounds__(256) k_finalize_batched(const BatchTable t) {
     const int64_t total = t.gauss_prefix[t.count];
     for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
          x += int64_t(gridDim.x) * blockDim.x) {
         const int i = find_item(t.gauss_prefix, t.count, x);
-        finalize_one<DET>(t.items[i], x - t.gauss_prefix[i]);
+        finalize_one(t.items[i], x - t.gauss_prefix[i]);
+    }
+}
+
+// One warp per Gaussian of every volume (deterministic backward).
+__global__ void __launch_bounds__(256) k_gather_det_batched(const BatchTable t) {
+    const int64_t total = t.gauss_prefix[t.count];
+    const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t x = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; x < total; x += warps) {
+        const int i = find_item(t.gauss_prefix, t.count, x);  // warp-uniform
+        gather_det_warp(t.items[i], x - t.gauss_prefix[i], threadIdx.x & 31);
     }
 }
 
@@ -975,6 +1013,9 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     a.gvol = grad_volume;
     a.accum = mat<float>(ws_gauss, G.accum);
     a.partials = det ? mat<float>(ws_pairs, P.partials) : nullptr;
+    a.offsets = cat<int64_t>(ws_gauss, G.offsets);
+    a.boxes = cat<int4>(ws_gauss, G.box);
+    a.capacity = capacity;
     if (det) {
         if (capacity > 0)
             GSV_CUDA_TRY(cudaMemsetAsync(a.partials, 0, size_t(capacity) * kMomStride * sizeof(float), st));
@@ -999,9 +1040,11 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     }
     a.prm = *p;
     a.grd = *grads;
-    a.boxes = cat<int4>(ws_gauss, G.box);
-    if (det) k_finalize<true><<<grid_for(n, 256), 256, 0, st>>>(a);
-    else k_finalize<false><<<grid_for(n, 256), 256, 0, st>>>(a);
+    if (det) {
+        k_gather_det<<<grid_for(n * 32, 256), 256, 0, st>>>(a);
+        GSV_LAUNCH_CHECK();
+    }
+    k_finalize<<<grid_for(n, 256), 256, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }
@@ -1113,6 +1156,8 @@ int gsv_batch_setup(const gsv_batch_item* items, int count, int flags, void* ws_
         a.prm = it.params;
         a.grd = it.grads;
         a.boxes = cat<int4>(it.ws_gauss, G.box);
+        a.offsets = cat<int64_t>(it.ws_gauss, G.offsets);
+        a.capacity = it.capacity;
         a.chunk = (it.chunk >= 1 && it.chunk <= 32) ? it.chunk : 32;
         host[i] = a;
         tp[i + 1] = tp[i] + ntiles;
@@ -1188,8 +1233,12 @@ int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream) {
     if (det) k_backward8_batched<true><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<true>), kThreads), kThreads, 0, st>>>(t);
     else k_backward8_batched<false><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<false>), kThreads), kThreads, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
-    if (det) k_finalize_batched<true><<<grid, 256, 0, st>>>(t);
-    else k_finalize_batched<false><<<grid, 256, 0, st>>>(t);
+    if (det) {
+        k_gather_det_batched<<<persistent_grid(reinterpret_cast<const void*>(k_gather_det_batched), 256), 256, 0,
+                               st>>>(t);
+        GSV_LAUNCH_CHECK();
+    }
+    k_finalize_batched<<<grid, 256, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }
