@@ -267,6 +267,11 @@ __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, in
         }
     }
     const unsigned keep = __ballot_sync(kFull, bits != 0);
+    if (DET && lane < cnt && !bits) {  // dropped pair: its partial is zero
+        float4* dst = reinterpret_cast<float4*>(a.partials +
+                                                emission_index(a, gid, d0 >> 3, h0 >> 3, w0 >> 3) * kMomStride);
+        dst[0] = dst[1] = dst[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     if (bits) {
         const int pos = __popc(keep & ((1u << lane) - 1u));
         S.rec[pos] = r;
@@ -500,7 +505,13 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                     }
                 }
             }
-            if (!wany) continue;
+            if (!wany) {  // no included voxel here: the pair's partial is zero
+                if (DET && lane == 0) {
+                    float4* dst = reinterpret_cast<float4*>(a.partials + int64_t(S.pidx[j]) * kMomStride);
+                    dst[0] = dst[1] = dst[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                continue;
+            }
             float v[16];
             float R0s = 0.f, R1s = 0.f, R2s = 0.f, S1 = 0.f, S2 = 0.f, S3 = 0.f;
 #pragma unroll
@@ -873,17 +884,15 @@ __global__ void __launch_bounds__(kThreads, 6) k_backward8_batched(const BatchTa
     }
 }
 
-// Zero the gradient accumulators (or deterministic partials) of every volume.
+// Zero the atomic accumulators of every volume (the deterministic backward
+// writes every listed pair's partial and needs no clearing).
 __global__ void k_zero_batched(const BatchTable t) {
-    const int64_t total = t.det ? t.cap_prefix[t.count] * kMomStride : t.gauss_prefix[t.count] * kMomStride;
-    const int64_t* prefix = t.det ? t.cap_prefix : t.gauss_prefix;
+    const int64_t total = t.det ? 0 : t.gauss_prefix[t.count] * kMomStride;
     for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
          x += int64_t(gridDim.x) * blockDim.x) {
         const int64_t row = x / kMomStride;
-        const int i = find_item(prefix, t.count, row);
-        const int64_t local = x - prefix[i] * kMomStride;
-        float* dst = t.det ? t.items[i].partials : t.items[i].accum;
-        dst[local] = 0.0f;
+        const int i = find_item(t.gauss_prefix, t.count, row);
+        t.items[i].accum[x - t.gauss_prefix[i] * kMomStride] = 0.0f;
     }
 }
 
@@ -1016,12 +1025,9 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     a.offsets = cat<int64_t>(ws_gauss, G.offsets);
     a.boxes = cat<int4>(ws_gauss, G.box);
     a.capacity = capacity;
-    if (det) {
-        if (capacity > 0)
-            GSV_CUDA_TRY(cudaMemsetAsync(a.partials, 0, size_t(capacity) * kMomStride * sizeof(float), st));
-    } else {
-        GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
-    }
+    // deterministic: every listed pair's partial is written (zero where the
+    // pair adds nothing), so only the atomic accumulators need clearing
+    if (!det) GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
     if (tuning) {
         a.chunk = tuning->chunk;
         a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
