@@ -84,6 +84,10 @@ SIGNATURES = {
     "gsv_mlp_gemm": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
                                     ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                     _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _vp, _vp, _vp]),
+    "gsv_sense_workspace_bytes": (_sz, []),
+    "gsv_sense_expand": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
+    "gsv_sense_residual": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _sz, _vp]),
+    "gsv_sense_adjoint": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),
 }

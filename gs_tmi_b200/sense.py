@@ -60,6 +60,7 @@ class FitConfig:
     eval_every: int = 100
     seed: int = 0
     capturable_adam: bool = False  # device-side LR/bias correction (what fit_graph uses)
+    fused_sense: bool = True       # data term through the fused SENSE kernels (sense_data_term)
 
 
 # ---------------------------------------------------------------------------
@@ -100,6 +101,62 @@ def ssim3d(pred: torch.Tensor, target: torch.Tensor, data_range: Optional[float]
     sxy = (mu(x * y) - mx * my) * cov
     s = ((2 * mx * my + c1) * (2 * sxy + c2)) / ((mx * mx + my * my + c1) * (sxx + syy + c2))
     return float(s.mean())
+
+
+class _SenseDataTerm(torch.autograd.Function):
+    """sum_c || M * fft3c(S_c x) - y_c ||^2 with the coil product, the FFT
+    shifts, the mask, the residual, its square sum and the adjoint coil sum
+    in the library's fused kernels (gsv_sense_*) and the FFTs in torch.fft."""
+
+    @staticmethod
+    def forward(ctx, vol, S, mask, ku, ws):
+        from ._lib import check, lib
+
+        nc, (d, h, w) = S.shape[0], vol.shape
+        st = torch.cuda.current_stream(vol.device).cuda_stream
+        X = torch.empty_like(S)
+        check(lib.gsv_sense_expand(vol.data_ptr(), S.data_ptr(), nc, d, h, w, X.data_ptr(), st), "gsv_sense_expand")
+        K = torch.fft.fftn(X, dim=(-3, -2, -1), norm="ortho")
+        loss = torch.empty((), device=vol.device)
+        check(lib.gsv_sense_residual(K.data_ptr(), mask.data_ptr(), ku.data_ptr(), nc, d, h, w, loss.data_ptr(),
+                                     ws.data_ptr(), ws.numel(), st), "gsv_sense_residual")
+        ctx.save_for_backward(K, S)  # K now holds dL/dK = 2 M R
+        return loss
+
+    @staticmethod
+    def backward(ctx, gout):
+        from ._lib import check, lib
+
+        K, S = ctx.saved_tensors
+        nc, (d, h, w) = S.shape[0], S.shape[1:]
+        with torch.cuda.device(K.device):  # the autograd thread may have no current context
+            G = torch.fft.ifftn(K, dim=(-3, -2, -1), norm="ortho")
+            vg = torch.empty((d, h, w), dtype=torch.complex64, device=K.device)
+            check(lib.gsv_sense_adjoint(G.data_ptr(), S.data_ptr(), nc, d, h, w, vg.data_ptr(),
+                                        torch.cuda.current_stream(K.device).cuda_stream), "gsv_sense_adjoint")
+            return vg * gout, None, None, None, None
+
+
+def sense_workspace(device) -> torch.Tensor:
+    from ._lib import lib
+
+    return torch.empty(int(lib.gsv_sense_workspace_bytes()), dtype=torch.uint8, device=device)
+
+
+def sense_data_term(vol: torch.Tensor, S: torch.Tensor, mask: torch.Tensor, ku: torch.Tensor,
+                    ws: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Scalar data term of the plain loss (trainer.py:256-268), differentiable
+    in `vol` (complex64 [d,h,w]); S, ku complex64 [C,d,h,w], mask float32
+    [d,h,w], all contiguous on the same GPU."""
+    if ws is None:
+        ws = sense_workspace(vol.device)
+    return _SenseDataTerm.apply(vol.contiguous(), S, mask, ku, ws)
+
+
+def data_term_reference(vol, S, mask_c, ku):
+    """The same data term op by op in torch (the reference's formulation)."""
+    diff = fft3c(vol.unsqueeze(0) * S) * mask_c - ku
+    return diff.real.square().sum() + diff.imag.square().sum()
 
 
 def hard_data_consistency(vol, S, mask, ku):
@@ -265,8 +322,11 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
 
         voxelizer = TileVoxelizer(shape, tile_size=cfg.tile_size, device=str(dev), deterministic=cfg.deterministic)
     S = case.sensitivity_maps.to(dev)
-    mask = case.mask.to(dev)
-    ku = case.kspace_undersampled.to(dev)
+    mask = case.mask.to(dev).float().contiguous()
+    ku = case.kspace_undersampled.to(dev).to(torch.complex64).contiguous()
+    S = S.to(torch.complex64).contiguous()
+    fused = cfg.fused_sense and dev.type == "cuda"
+    ws = sense_workspace(dev) if fused else None
     gt = case.ground_truth.to(dev)
     p = GaussianParams(init, dev)
     lrs = [cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr, cfg.density_lr]
@@ -285,8 +345,7 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
         vol = voxelizer(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
         if isinstance(vol, tuple):
             vol = torch.complex(vol[0], vol[1])
-        diff = fft3c(vol.unsqueeze(0) * S) * mask_c - ku
-        loss = diff.real.square().sum() + diff.imag.square().sum()
+        loss = sense_data_term(vol, S, mask, ku, ws) if fused else data_term_reference(vol, S, mask_c, ku)
         if cfg.tv_weight > 0:
             loss = loss + cfg.tv_weight * magnitude_tv(vol)
         loss.backward()
@@ -373,6 +432,7 @@ class _GraphedStep:
         self.live = p.tensors() + self.state_tensors
         self.snap = [torch.empty_like(t) for t in self.live]
         self.S, self.mask_c, self.ku = S, mask_c, ku
+        self.ws = sense_workspace(dev) if cfg.fused_sense else None
         self.graph = None
         self.stream = torch.cuda.Stream(dev)
 
@@ -382,8 +442,10 @@ class _GraphedStep:
             t.grad.zero_()
         p = self.p
         vol = self.svox(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
-        diff = fft3c(vol.unsqueeze(0) * self.S) * self.mask_c - self.ku
-        loss = diff.real.square().sum() + diff.imag.square().sum()
+        if self.cfg.fused_sense:
+            loss = sense_data_term(vol, self.S, self.mask_c[0], self.ku, self.ws)
+        else:
+            loss = data_term_reference(vol, self.S, self.mask_c, self.ku)
         if self.cfg.tv_weight > 0:
             loss = loss + self.cfg.tv_weight * magnitude_tv(vol)
         loss.backward()
@@ -451,9 +513,9 @@ def fit_graph(case: MRICase, init: GaussianSet, cfg: FitConfig, device="cuda:0",
     dev = torch.device(device)
     shape = tuple(case.ground_truth.shape)
     vox = TileVoxelizer(shape, tile_size=cfg.tile_size, device=str(dev), deterministic=cfg.deterministic)
-    S = case.sensitivity_maps.to(dev)
-    mask = case.mask.to(dev)
-    ku = case.kspace_undersampled.to(dev)
+    S = case.sensitivity_maps.to(dev).to(torch.complex64).contiguous()
+    mask = case.mask.to(dev).float().contiguous()
+    ku = case.kspace_undersampled.to(dev).to(torch.complex64).contiguous()
     gt = case.ground_truth.to(dev)
     mask_c = mask.unsqueeze(0)
     p = GaussianParams(init, dev)

@@ -257,6 +257,28 @@ GSV_API int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const vo
                          void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, float* col_sum,
                          int* error, void* stream);
 
+/* ---- fused SENSE data term around the FFTs ---------------------------- */
+
+/* Replace the elementwise torch ops of the plain loss's data term
+ * (V/trainers/trainer.py:256-268, V/losses/losses.py:18-26):
+ *   L = sum_c || M * fft3c(S_c x) - y_c ||^2,  fft3c = fftshift o fftn(ortho) o ifftshift,
+ * with the FFTs left to the caller (torch.fft / cuFFT) and the shifts folded
+ * into the indexing.  Complex arrays are interleaved complex64; x, M are
+ * [d,h,w], S, y and the coil images [ncoils,d,h,w].
+ *   gsv_sense_expand  : out = ifftshift(S x)                  (then out <- fftn(out))
+ *   gsv_sense_residual: kspace holds fftn(out); *loss = L (device float, fixed-order sum)
+ *                       and kspace <- 2 M R, the gradient of L w.r.t. it    (then ifftn)
+ *   gsv_sense_adjoint : volume_grad = sum_c conj(S_c) fftshift-inverse(ifftn(2 M R))_c,
+ *                       dL/dx in torch's complex-gradient convention.
+ * ws: gsv_sense_workspace_bytes() bytes of device scratch for the loss sum. */
+GSV_API size_t gsv_sense_workspace_bytes(void);
+GSV_API int gsv_sense_expand(const float* volume, const float* coils, int32_t ncoils, int32_t d, int32_t h, int32_t w,
+                             float* out, void* stream);
+GSV_API int gsv_sense_residual(float* kspace, const float* mask, const float* measured, int32_t ncoils, int32_t d,
+                               int32_t h, int32_t w, float* loss, void* ws, size_t ws_bytes, void* stream);
+GSV_API int gsv_sense_adjoint(const float* kgrad_image, const float* coils, int32_t ncoils, int32_t d, int32_t h,
+                              int32_t w, float* volume_grad, void* stream);
+
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 
 /* centers [n,3] voxel units, cov_inv [n,3,3] normalised units (symmetric;

@@ -6,6 +6,7 @@ own CUDA kernels on the same seeded inputs (bar: final NMSE and SSIM within
 GSV_RECON_FULL=1 additionally runs the 128x128x96 / 8-coil / R=6 / 50k->500k /
 2000-iteration plain reconstruction with both voxelizers and writes wall
 times and metrics to $GSV_REPORT_DIR/recon_128x128x96.json."""
+import dataclasses
 import json
 import os
 
@@ -81,6 +82,9 @@ def test_full_plain_reconstruction_128x128x96(cuda_device):
     r2 = sense.fit(case, init, cfg, voxelizer=RefVoxelizer(shape), device=str(cuda_device), eval_ssim=True)
     report["reference_kernels_rerun"] = {"seconds": r2.seconds, "final_nmse": r2.final_nmse,
                                          "final_ssim": r2.final_ssim, "n_points": r2.params.n}
+    r3 = sense.fit(case, init, dataclasses.replace(cfg, fused_sense=False), device=str(cuda_device), eval_ssim=False)
+    report["this_build_torch_data_term"] = {"seconds": r3.seconds, "final_nmse": r3.final_nmse,
+                                            "n_points": r3.params.n}
     report["reference_rerun_nmse_rel_diff"] = r2.final_nmse / report["reference_kernels"]["final_nmse"] - 1
     report["wall_speedup"] = report["reference_kernels"]["seconds"] / report["this_build"]["seconds"]
     report["nmse_rel_diff"] = report["this_build"]["final_nmse"] / report["reference_kernels"]["final_nmse"] - 1
