@@ -137,6 +137,35 @@ class _SenseDataTerm(torch.autograd.Function):
             return vg * gout, None, None, None, None
 
 
+class _MagnitudeTV(torch.autograd.Function):
+    """TV(|x|) (losses.py:18-26) with its gradient from the same pass of the
+    library kernel (gsv_tv_magnitude)."""
+
+    @staticmethod
+    def forward(ctx, vol, ws):
+        from ._lib import check, lib
+
+        d, h, w = vol.shape
+        loss = torch.empty((), device=vol.device)
+        grad = torch.empty_like(vol)
+        check(lib.gsv_tv_magnitude(vol.data_ptr(), d, h, w, loss.data_ptr(), grad.data_ptr(), ws.data_ptr(),
+                                   ws.numel(), torch.cuda.current_stream(vol.device).cuda_stream), "gsv_tv_magnitude")
+        ctx.save_for_backward(grad)
+        return loss
+
+    @staticmethod
+    def backward(ctx, gout):
+        (grad,) = ctx.saved_tensors
+        return grad * gout, None
+
+
+def magnitude_tv_fused(vol: torch.Tensor, ws: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """magnitude_tv on the GPU in one kernel (value and gradient)."""
+    if ws is None:
+        ws = sense_workspace(vol.device)
+    return _MagnitudeTV.apply(vol.contiguous(), ws)
+
+
 def sense_workspace(device) -> torch.Tensor:
     from ._lib import lib
 
@@ -327,6 +356,7 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
     S = S.to(torch.complex64).contiguous()
     fused = cfg.fused_sense and dev.type == "cuda"
     ws = sense_workspace(dev) if fused else None
+    ws_tv = sense_workspace(dev) if fused else None
     gt = case.ground_truth.to(dev)
     p = GaussianParams(init, dev)
     lrs = [cfg.position_lr, cfg.scale_lr, cfg.rotation_lr, cfg.density_lr, cfg.density_lr]
@@ -347,7 +377,7 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
             vol = torch.complex(vol[0], vol[1])
         loss = sense_data_term(vol, S, mask, ku, ws) if fused else data_term_reference(vol, S, mask_c, ku)
         if cfg.tv_weight > 0:
-            loss = loss + cfg.tv_weight * magnitude_tv(vol)
+            loss = loss + cfg.tv_weight * (magnitude_tv_fused(vol, ws_tv) if fused else magnitude_tv(vol))
         loss.backward()
         pos_grad = p.positions.grad.detach().clone()
         if cfg.max_grad_norm > 0:
@@ -433,6 +463,7 @@ class _GraphedStep:
         self.snap = [torch.empty_like(t) for t in self.live]
         self.S, self.mask_c, self.ku = S, mask_c, ku
         self.ws = sense_workspace(dev) if cfg.fused_sense else None
+        self.ws_tv = sense_workspace(dev) if cfg.fused_sense else None
         self.graph = None
         self.stream = torch.cuda.Stream(dev)
 
@@ -447,7 +478,8 @@ class _GraphedStep:
         else:
             loss = data_term_reference(vol, self.S, self.mask_c, self.ku)
         if self.cfg.tv_weight > 0:
-            loss = loss + self.cfg.tv_weight * magnitude_tv(vol)
+            tv = magnitude_tv_fused(vol, self.ws_tv) if self.cfg.fused_sense else magnitude_tv(vol)
+            loss = loss + self.cfg.tv_weight * tv
         loss.backward()
         self.pos_grad.copy_(p.positions.grad)
         if self.cfg.max_grad_norm > 0:

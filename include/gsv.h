@@ -278,6 +278,13 @@ GSV_API int gsv_sense_residual(float* kspace, const float* mask, const float* me
                                int32_t h, int32_t w, float* loss, void* ws, size_t ws_bytes, void* stream);
 GSV_API int gsv_sense_adjoint(const float* kgrad_image, const float* coils, int32_t ncoils, int32_t d, int32_t h,
                               int32_t w, float* volume_grad, void* stream);
+/* Magnitude total variation of the plain loss (V/losses/losses.py:18-26, used at
+ * V/trainers/trainer.py:261-274):
+ * *loss = sum over the three axes of | |x|[i + e_a] - |x|[i] | (device float,
+ * fixed-order sum) and grad = dTV/dx in torch's complex convention, one pass.
+ * ws as for gsv_sense_residual. */
+GSV_API int gsv_tv_magnitude(const float* volume, int32_t d, int32_t h, int32_t w, float* loss, float* grad, void* ws,
+                             size_t ws_bytes, void* stream);
 
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 

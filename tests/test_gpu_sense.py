@@ -47,3 +47,18 @@ def test_fused_data_term_in_a_fit(cuda_device):
         assert r.final_nmse < r.history[0]["nmse"]
         out.append(r.final_nmse)
     assert abs(out[0] - out[1]) <= 2e-2 * out[1]
+
+
+@pytest.mark.parametrize("shape", [(16, 12, 10), (13, 11, 9), (1, 7, 5)])
+def test_fused_tv_matches_torch(shape, cuda_device):
+    g = torch.Generator().manual_seed(sum(shape))
+    vol = _crand(shape, g, cuda_device)
+    vol[0, 0, 0] = 0  # |x| = 0: zero gradient, as torch's abs backward
+    v1 = vol.clone().requires_grad_(True)
+    l1 = sense.magnitude_tv_fused(v1)
+    (3 * l1).backward()
+    v2 = vol.clone().requires_grad_(True)
+    l2 = sense.magnitude_tv(v2)
+    (3 * l2).backward()
+    assert abs(float(l1.detach()) - float(l2.detach())) <= 1e-5 * abs(float(l2.detach()))
+    assert float((v1.grad - v2.grad).abs().norm() / v2.grad.abs().norm()) < 1e-5
