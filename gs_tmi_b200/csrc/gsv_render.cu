@@ -162,6 +162,50 @@ __device__ __forceinline__ float warp_reduce_scatter16(float v[16], int lane) {
     return v[0] + __shfl_xor_sync(kFull, v[0], 1);
 }
 
+// Reduce-scatter of the 11 moments (v[11] must be 0) over the warp in 13
+// shuffles: afterwards lanes l and l^1 hold the warp total of moment
+// moment12(l) = 6*b4 + 3*b3 + 2*b2 + b1 (b_k = bit k of l), where a value of
+// 3 for 2*b2 + b1 is padding (the moment then reads as -1).
+__device__ __forceinline__ float warp_reduce_scatter12(float v[12], int lane) {
+    {
+        const bool hi = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const float send = hi ? v[i] : v[i + 6];
+            const float keep = hi ? v[i + 6] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 16);
+        }
+    }
+    {
+        const bool hi = lane & 8;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float send = hi ? v[i] : v[i + 3];
+            const float keep = hi ? v[i + 3] : v[i];
+            v[i] = keep + __shfl_xor_sync(kFull, send, 8);
+        }
+    }
+    {
+        const bool hi = lane & 4;  // group of 3 -> pairs {0, 1} and {2, pad}
+        const float send0 = hi ? v[0] : v[2], keep0 = hi ? v[2] : v[0];
+        const float send1 = hi ? v[1] : 0.f, keep1 = hi ? 0.f : v[1];
+        v[0] = keep0 + __shfl_xor_sync(kFull, send0, 4);
+        v[1] = keep1 + __shfl_xor_sync(kFull, send1, 4);
+    }
+    {
+        const bool hi = lane & 2;
+        const float send = hi ? v[0] : v[1];
+        const float keep = hi ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(kFull, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(kFull, v[0], 1);
+}
+
+__device__ __forceinline__ int moment12(int lane) {
+    const int sub = ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+    return sub == 3 ? -1 : ((lane >> 4) & 1) * 6 + ((lane >> 3) & 1) * 3 + sub;
+}
+
 // Compat outputs for one (tile, Gaussian): every lane holds `tot` (lane 2i
 // holds moment i); lanes 0..13 issue one atomic each.
 __device__ __forceinline__ void compat_emit(const RenderArgs& a, const Rec& g, int gid, float tot,
@@ -534,18 +578,19 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
             v[8] = (e1 * e1) * R0s;
             v[9] = e1 * R1s;
             v[10] = R2s;
-#pragma unroll
-            for (int i = 11; i < 16; ++i) v[i] = 0.f;
-            const float tot = warp_reduce_scatter16(v, lane);
             const int gid = S.gid[j];
             if (COMPAT) {
-                compat_emit(a, g, gid, tot, lane, ih);
-            } else if (DET) {
-                if (!(lane & 1) && (lane >> 1) < kMom)
-                    a.partials[int64_t(S.pidx[j]) * kMomStride + (lane >> 1)] = tot;
+#pragma unroll
+                for (int i = 11; i < 16; ++i) v[i] = 0.f;
+                compat_emit(a, g, gid, warp_reduce_scatter16(v, lane), lane, ih);
             } else {
-                if (!(lane & 1) && (lane >> 1) < kMom)
-                    atomicAdd(a.accum + int64_t(gid) * kMomStride + (lane >> 1), tot);
+                v[11] = 0.f;
+                const float tot = warp_reduce_scatter12(v, lane);
+                const int mi = moment12(lane);
+                if (!(lane & 1) && mi >= 0 && mi < kMom) {
+                    if (DET) a.partials[int64_t(S.pidx[j]) * kMomStride + mi] = tot;
+                    else atomicAdd(a.accum + int64_t(gid) * kMomStride + mi, tot);
+                }
             }
         }
         __syncwarp();
