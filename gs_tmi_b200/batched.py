@@ -11,6 +11,9 @@ tile) work items from an atomic counter (``gsv_forward_batched`` /
 * ``StaticBatch`` -- fixed Gaussian counts and pair capacities: binning,
   forward and backward only enqueue work, so a whole batched iteration can
   be captured in a CUDA graph and replayed.
+* ``BatchedRecon`` -- a whole plain-reconstruction iteration over the batch
+  (SENSE data term and TV per volume, Adam over all parameters) on top of a
+  StaticBatch, also only enqueued work.
 """
 from __future__ import annotations
 
@@ -153,3 +156,94 @@ class StaticBatch:
 
     def overflowed(self) -> List[bool]:
         return [bool(int(p.flags_dev.item()) & _lib.GSV_FLAG_CAPACITY_OVERFLOW) for p in self.plans]
+
+
+class BatchedRecon:
+    """One plain-reconstruction iteration over several volumes at once:
+    scales = exp(log-scales), per-volume binning, ONE persistent forward
+    launch, per volume the fused SENSE data term and magnitude TV (their
+    volume gradients written straight into the batch's upstream gradients),
+    ONE persistent backward launch, the chain rule to the log-scales, a
+    per-volume gradient-norm clip and one fused Adam step over every
+    volume's parameters.  ``step()`` only enqueues work, so one CUDA graph
+    captures the whole iteration.
+
+    cases: synthetic.MRICase per volume (on any device); inits: GaussianSet
+    per volume; capacities: static pair capacity per volume."""
+
+    def __init__(self, cases, inits, capacities, device="cuda:0", deterministic: bool = False, chunks=None,
+                 tv_weight: float = 0.1, max_grad_norm: float = 1.0, lrs=(1e-3, 5e-3, 1e-3, 1e-2, 1e-2)):
+        from . import sense
+
+        dev = torch.device(device)
+        self.device = dev
+        shapes = [tuple(c.ground_truth.shape) for c in cases]
+        self.sb = StaticBatch(shapes, [g.n for g in inits], capacities, device=str(dev),
+                              deterministic=deterministic, chunks=chunks)
+        self.tv_weight, self.max_grad_norm = float(tv_weight), float(max_grad_norm)
+        self.S = [c.sensitivity_maps.to(dev).to(torch.complex64).contiguous() for c in cases]
+        self.mask = [c.mask.to(dev).float().contiguous() for c in cases]
+        self.ku = [c.kspace_undersampled.to(dev).to(torch.complex64).contiguous() for c in cases]
+        self.ws = sense.sense_workspace(dev)
+        self.tv_grad = [torch.empty_like(v) for v in self.sb.volumes]
+        self.data_loss = [torch.zeros((), device=dev) for _ in cases]
+        self.tv_loss = [torch.zeros((), device=dev) for _ in cases]
+        groups = [[] for _ in range(5)]
+        self.leaves = []
+        for i, gs in enumerate(inits):
+            pos, scl, rot, dr, di = self.sb.params[i]
+            pos.copy_(gs.positions.to(dev))
+            rot.copy_(gs.rotations.to(dev))
+            dr.copy_(gs.density_r.to(dev))
+            di.copy_(gs.density_i.to(dev))
+            log_s = torch.log(gs.scales.to(dev).clamp_min(1e-12))
+            leaves = [torch.nn.Parameter(pos), torch.nn.Parameter(log_s), torch.nn.Parameter(rot),
+                      torch.nn.Parameter(dr), torch.nn.Parameter(di)]
+            gpos, gscl, grot, gdr, gdi = self.sb.grads[i]
+            # the batched backward writes these buffers in place: they are the gradients
+            leaves[0].grad, leaves[2].grad, leaves[3].grad, leaves[4].grad = gpos, grot, gdr, gdi
+            leaves[1].grad = torch.zeros_like(log_s)
+            for k, t in enumerate(leaves):
+                groups[k].append(t)
+            self.leaves.append(leaves)
+        self.lrs = [torch.tensor(float(v), device=dev) for v in lrs]
+        self.opt = torch.optim.Adam([{"params": g, "lr": lr} for g, lr in zip(groups, self.lrs)], fused=True,
+                                    capturable=True)
+
+    def step(self):
+        sb = self.sb
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        with torch.no_grad():
+            for i, leaves in enumerate(self.leaves):
+                torch.exp(leaves[1], out=sb.params[i][1])
+            sb.bin()
+            sb.forward()
+            for i, vol in enumerate(sb.volumes):
+                d, h, w = vol.shape
+                nc = self.S[i].shape[0]
+                X = torch.empty_like(self.S[i])
+                check(lib.gsv_sense_expand(vol.data_ptr(), self.S[i].data_ptr(), nc, d, h, w, X.data_ptr(), st),
+                      "gsv_sense_expand")
+                K = torch.fft.fftn(X, dim=(-3, -2, -1), norm="ortho")
+                check(lib.gsv_sense_residual(K.data_ptr(), self.mask[i].data_ptr(), self.ku[i].data_ptr(), nc, d,
+                                             h, w, self.data_loss[i].data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+                                             st), "gsv_sense_residual")
+                G = torch.fft.ifftn(K, dim=(-3, -2, -1), norm="ortho")
+                gv = sb.grad_volumes[i]
+                check(lib.gsv_sense_adjoint(G.data_ptr(), self.S[i].data_ptr(), nc, d, h, w, gv.data_ptr(), st),
+                      "gsv_sense_adjoint")
+                if self.tv_weight > 0:
+                    check(lib.gsv_tv_magnitude(vol.data_ptr(), d, h, w, self.tv_loss[i].data_ptr(),
+                                               self.tv_grad[i].data_ptr(), self.ws.data_ptr(), self.ws.numel(), st),
+                          "gsv_tv_magnitude")
+                    gv.add_(self.tv_grad[i], alpha=self.tv_weight)
+            sb.backward()
+            for i, leaves in enumerate(self.leaves):
+                torch.mul(sb.grads[i][1], sb.params[i][1], out=leaves[1].grad)  # d/d log s = d/ds * s
+                if self.max_grad_norm > 0:
+                    torch.nn.utils.clip_grad_norm_(leaves, self.max_grad_norm, foreach=True)
+        self.opt.step()
+
+    def losses(self) -> List[float]:
+        """Per-volume data + tv_weight * TV of the last step (synchronises)."""
+        return [float(a) + self.tv_weight * float(b) for a, b in zip(self.data_loss, self.tv_loss)]

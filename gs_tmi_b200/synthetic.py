@@ -221,16 +221,20 @@ class MRICase:
 
 
 def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise_rel: float = 1e-3,
-             seed: int = 0) -> MRICase:
+             seed: int = 0, device=None) -> MRICase:
     """Synthetic multi-coil acquisition: phantom x coils -> fft3c -> mask +
-    complex noise sigma = noise_rel * max|k| -> SENSE-combined zero-filled."""
-    x = ellipsoid_phantom(shape, seed=seed)
-    S = ring_coils(shape, n_coils, seed=seed + 1)
+    complex noise sigma = noise_rel * max|k| -> SENSE-combined zero-filled.
+    `device`: where the FFTs and the noise are computed (and the case lives);
+    the default, the CPU, is the reference generator of all seeded cases."""
+    dev = torch.device(device) if device is not None else torch.device("cpu")
+    x = ellipsoid_phantom(shape, seed=seed).to(dev)
+    S = ring_coils(shape, n_coils, seed=seed + 1).to(dev)
     k = fft3c(S * x.unsqueeze(0))
-    g = torch.Generator().manual_seed(seed + 2)
+    g = torch.Generator(device=dev).manual_seed(seed + 2)
     sigma = noise_rel * float(k.abs().max())
-    noise = torch.complex(torch.randn(k.shape, generator=g), torch.randn(k.shape, generator=g)) * sigma
-    m = variable_density_mask(shape, accel, calib, seed=seed + 3)
+    noise = torch.complex(torch.randn(k.shape, generator=g, device=dev),
+                          torch.randn(k.shape, generator=g, device=dev)) * sigma
+    m = variable_density_mask(shape, accel, calib, seed=seed + 3).to(dev)
     ku = (k + noise) * m.unsqueeze(0)
     zf = (torch.conj(S) * ifft3c(ku)).sum(0)
     return MRICase(x, S, m, ku.to(torch.complex64), zf.to(torch.complex64))
