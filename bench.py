@@ -198,7 +198,10 @@ def run_batched_recon(args, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", 0))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    cases, inits, caps, evals = [], [], [], 0
+    from gs_tmi_b200.autotune import WHOLE_TILE, Autotuner
+
+    tuner = Autotuner()
+    cases, inits, caps, chunks, evals = [], [], [], [], 0
     for i, (shape, n) in enumerate(BATCH12):
         case = synthetic.mri_case(shape, n_coils=BATCH12_COILS[i], accel=BATCH12_ACCEL[i], calib=24, seed=100 + i,
                                   device=dev)
@@ -207,6 +210,7 @@ def run_batched_recon(args, rank, world, dist):
         params = tuple(t.to(dev) for t in gs.tensors())
         plan = __import__("gs_tmi_b200").prepare_and_bin(params, vz._shape)
         caps.append(int(plan.total * 2) + 4096)  # the Gaussians move during the timed iterations
+        chunks.append(32 if args.no_autotune else tuner.pick(plan, params, WHOLE_TILE).chunk)
         tr_ptr, _ = plan.views()
         nt = lib_num_tiles(vz._shape)
         off = tr_ptr - plan.ws_gauss.data_ptr()
@@ -215,7 +219,7 @@ def run_batched_recon(args, rank, world, dist):
         cases.append(case)
         inits.append(gs)
         del plan
-    rec = batched.BatchedRecon(cases, inits, caps, device=str(dev), deterministic=args.deterministic)
+    rec = batched.BatchedRecon(cases, inits, caps, device=str(dev), deterministic=args.deterministic, chunks=chunks)
     side = torch.cuda.Stream(dev)
     side.wait_stream(torch.cuda.current_stream(dev))
     with torch.cuda.stream(side):
@@ -256,6 +260,7 @@ def run_batched_recon(args, rank, world, dist):
            "config": {"workload": "batch12_recon", "volumes": [list(s) for s, _ in BATCH12],
                       "gaussians": [n for _, n in BATCH12], "coils": BATCH12_COILS,
                       "acceleration": [round(a, 2) for a in BATCH12_ACCEL], "tile_size": TILE,
+                      "autotuned_chunk_per_volume": chunks,
                       "evals_per_step": evals, "deterministic": bool(args.deterministic),
                       "iteration": "exp(log-scales), binning x12, 1 persistent forward, SENSE data term + TV x12 "
                                    "(fused kernels + torch.fft), 1 persistent backward, clip x12, 1 fused Adam; "
