@@ -99,6 +99,30 @@ def test_full_plain_reconstruction_128x128x96(cuda_device):
     assert abs(report["nmse_rel_diff"]) <= max(0.03, 2 * spread)
 
 
+@pytest.mark.skipif(os.environ.get("GSV_RECON_LARGE") != "1", reason="set GSV_RECON_LARGE=1")
+def test_large_reconstruction_256x256x160(cuda_device):
+    """The large configuration end to end: 256x256x160, 16 coils, R=8,
+    200k intensity-seeded Gaussians growing towards 2M, deterministic
+    backward, 3000 iterations (GSV_RECON_LARGE_ITERS overrides).  Records
+    wall time, NMSE/SSIM and the Gaussian count to
+    $GSV_REPORT_DIR/recon_256x256x160.json; the fit must improve on its start."""
+    shape = (256, 256, 160)
+    iters = int(os.environ.get("GSV_RECON_LARGE_ITERS", "3000"))
+    case = synthetic.mri_case(shape, n_coils=16, accel=8.0, calib=24, seed=7, device=cuda_device)
+    init = synthetic.from_image_init(case.zero_filled.cpu(), 200_000, seed=7)
+    cfg = sense.FitConfig(iterations=iters, eval_every=250, max_points=2_000_000, deterministic=True)
+    r = sense.fit(case, init, cfg, device=str(cuda_device), eval_ssim=True)
+    report = {"seconds": r.seconds, "iterations": iters, "final_nmse": r.final_nmse, "final_ssim": r.final_ssim,
+              "final_psnr": r.final_psnr, "n_points": r.params.n, "history": r.history}
+    out = os.environ.get("GSV_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "recon_256x256x160.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    print(json.dumps({k: v for k, v in report.items() if k != "history"}))
+    assert r.final_nmse < r.history[0]["nmse"]
+
+
 def test_graph_fit_matches_eager(cuda_device):
     """Each iteration replayed from a CUDA graph computes exactly what the
     eager loop computes with the same (capturable) Adam and the deterministic
