@@ -29,6 +29,7 @@ import torch
 from ._lib import GsvGrads, GsvParams, GsvTuning, check, lib
 
 CANDIDATES: Tuple[Tuple[int, int], ...] = ((2, 32), (2, 16), (1, 32), (1, 16), (1, 8))
+TILE_SIZES: Tuple[int, ...] = (8, 4)  # binning tile edges compared by pick_tile_size
 WHOLE_TILE: Tuple[Tuple[int, int], ...] = ((2, 32), (2, 16), (2, 8))  # batched launches
 
 
@@ -104,6 +105,66 @@ class Autotuner:
             times[f"{rpl}/{chunk}"] = e0.elapsed_time(e1) / self.reps
         best = min(candidates, key=lambda c: times[f"{c[0]}/{c[1]}"])
         return best, times
+
+
+    def pick_tile_size(self, params, volume_shape, flags: int = 0) -> Tuple[int, GsvTuning, Dict[str, float]]:
+        """Binning tile edge for a problem: times one whole step (preprocess,
+        binning, forward, backward) at each edge of TILE_SIZES -- edge 8 with
+        its best execution shape (pick), edge 4 on the generic one-voxel-per-
+        thread kernels -- and keeps the fastest, cached like pick.  On a
+        cubic volume the edges include the same (voxel, Gaussian) pairs and
+        differ only by FP32 summation order.  On a non-cubic one the
+        reference's radius 3 max_j(s_j hs_j) can cut a rotated anisotropic
+        Gaussian at its tile box, and the cut depends on the edge: the
+        included pairs then differ, as they do in the reference."""
+        from .tile_voxelizer import _shape, prepare_and_bin
+
+        n = int(params[0].shape[0])
+        d, h, w = (int(x) for x in volume_shape)
+        k = f"{d}x{h}x{w}/n2^{int(math.ceil(math.log2(max(n, 1))))}/{'det' if flags & 1 else 'atomic'}/tile"
+        with self._lock:
+            if k in self.cache:
+                ts, rpl, chunk = self.cache[k]
+                return int(ts), GsvTuning(int(rpl), int(chunk)), self.timings.get(k, {})
+        times, tunings = {}, {}
+        dev = params[0].device
+        st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        vol = torch.empty((d, h, w), dtype=torch.complex64, device=dev)
+        gvol = torch.randn_like(vol)
+        outs = [torch.empty_like(t) for t in params]
+        gp = GsvParams(*(t.data_ptr() for t in params), n)
+        gg = GsvGrads(*(o.data_ptr() for o in outs))
+        for ts in TILE_SIZES:
+            shape = _shape((d, h, w), ts)
+            plan = prepare_and_bin(params, shape, flags)
+            tun = self.pick(plan, params) if ts == 8 else GsvTuning(2, 32)
+            tunings[ts] = tun
+
+            def run():
+                check(lib.gsv_prepare(ctypes.byref(gp), shape, _ptr(plan.ws_gauss), plan.gauss_bytes, None, st),
+                      "gsv_prepare")
+                check(lib.gsv_bin(shape, n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.pair_bytes,
+                                  plan.capacity, st), "gsv_bin")
+                check(lib.gsv_forward_ex(shape, n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
+                                         _ptr(vol), ctypes.byref(tun), st), "gsv_forward_ex")
+                check(lib.gsv_backward_ex(ctypes.byref(gp), shape, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs),
+                                          plan.capacity, _ptr(gvol), ctypes.byref(gg), flags, ctypes.byref(tun),
+                                          st), "gsv_backward_ex")
+
+            run()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(self.reps):
+                run()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times[str(ts)] = e0.elapsed_time(e1) / self.reps
+        best = min(TILE_SIZES, key=lambda t: times[str(t)])
+        with self._lock:
+            self.cache[k] = (best, tunings[best].rows_per_lane, tunings[best].chunk)
+            self.timings[k] = times
+            self.save()
+        return best, tunings[best], times
 
 
 _default: Optional[Autotuner] = None

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 import torch
 
+import gs_tmi_b200
 from gs_tmi_b200 import autotune, synthetic
 from gs_tmi_b200._lib import GSV_BACKWARD_DETERMINISTIC, GSV_TUNE_NO_CULL, GsvGrads, GsvParams, GsvTuning, check, lib
 from gs_tmi_b200.tile_voxelizer import _ptr, _shape, prepare_and_bin
@@ -110,3 +111,22 @@ def test_extent_cull_changes_nothing(kind, rpl, cuda_device):
     assert np.array_equal(on[0], off[0])
     for a, b, c in zip(on[1], off[1], off2[1]):
         assert rel(a, b) <= max(10 * rel(c, b), 1e-5)
+
+
+def test_tile_size_pick(tmp_path, cuda_device):
+    """The tile-edge choice (8^3 tiles with their execution shapes vs 4^3
+    tiles) is timed, cached, and both edges give the same volume on a cubic
+    volume.  (On a non-cubic one they need not: the reference's radius
+    3 max_j(s_j hs_j) pairs each scale with its own axis's half size, so a
+    rotated anisotropic Gaussian can reach past its tile box, and how much
+    of it a box keeps depends on the tile edge.)"""
+    shape = (40, 40, 40)
+    gs = synthetic.random_gaussians(4000, shape, seed=81)
+    params = tuple(t.to(cuda_device) for t in gs.tensors())
+    tuner = autotune.Autotuner(str(tmp_path / "tune.json"))
+    ts, tun, times = tuner.pick_tile_size(params, shape)
+    assert ts in autotune.TILE_SIZES and set(times) == {str(t) for t in autotune.TILE_SIZES}
+    assert tuner.pick_tile_size(params, shape)[0] == ts
+    v8 = gs_tmi_b200.voxelize(*params, shape, 8).cpu().numpy()
+    v4 = gs_tmi_b200.voxelize(*params, shape, 4).cpu().numpy()
+    assert rel(v4, v8) < FWD_TOL
