@@ -608,6 +608,207 @@ __global__ void __launch_bounds__(kThreads, RPL == 2 ? 6 : 7) k_backward8(const 
 }
 
 // ---------------------------------------------------------------------------
+// Tile edge 4: one warp per 4^3 tile (four tiles per CTA, no CTA barrier).
+// Lane l owns the voxel pair (d0 + l/8, h0 + (l/2)%4, w0 + 2(l%2) + {0,1});
+// the warp stages up to 32 of its tile's Gaussians at a time, drops those
+// whose tight extent misses the tile, and evaluates the rest with the row
+// form (A, B once per lane) and the warp-uniform exp skip of the 8^3
+// kernels.
+// ---------------------------------------------------------------------------
+
+struct __align__(16) WarpStage4 {
+    Rec rec[32];
+    int32_t gid[32];
+    int32_t pidx[32];  // deterministic backward: emission index of the pair
+};
+
+template <bool COMPAT, bool DET>
+__device__ __forceinline__ int stage4(const RenderArgs& a, WarpStage4& S, int base, int cnt, int lane, int d0,
+                                      int h0, int w0, const float ih[3]) {
+    Rec r;
+    int gid = 0;
+    bool keep = false;
+    if (lane < cnt) {
+        gid = __ldg(a.pair_ids + base + lane);
+        r = load_rec<COMPAT>(a, gid, ih);
+        keep = true;
+        if (a.cull) {
+            float4 x;
+            if (COMPAT) {
+                const float qc[6] = {r.q00, r.q01x2, r.q02x2, r.q11, r.q12x2, r.q22};
+                x = tight_extent(qc);
+            } else {
+                x = __ldg(a.ext + gid);
+            }
+            keep = __fsub_rn(r.c0, x.x) <= float(d0 + 3) && __fadd_rn(r.c0, x.x) >= float(d0) &&
+                   __fsub_rn(r.c1, x.y) <= float(h0 + 3) && __fadd_rn(r.c1, x.y) >= float(h0) &&
+                   __fsub_rn(r.c2, x.z) <= float(w0 + 3) && __fadd_rn(r.c2, x.z) >= float(w0);
+        }
+    }
+    const unsigned kept = __ballot_sync(kFull, keep);
+    int64_t e = 0;
+    if (DET && lane < cnt) e = emission_index(a, gid, d0 >> 2, h0 >> 2, w0 >> 2);
+    if (DET && lane < cnt && !keep) {  // dropped pair: its partial is zero
+        float4* dst = reinterpret_cast<float4*>(a.partials + e * kMomStride);
+        dst[0] = dst[1] = dst[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (keep) {
+        const int pos = __popc(kept & ((1u << lane) - 1u));
+        S.rec[pos] = r;
+        S.gid[pos] = gid;
+        if (DET) S.pidx[pos] = int32_t(e);
+    }
+    return __popc(kept);
+}
+
+template <bool COMPAT, bool PLANAR>
+__global__ void __launch_bounds__(kThreads) k_forward4(const RenderArgs a) {
+    __shared__ WarpStage4 stage[kWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t tile = int64_t(blockIdx.x) * kWarps + warp;
+    if (tile >= a.ntiles) return;  // warp-uniform; no CTA barrier below
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    const int2 rg = a.ranges[tile];
+    float ih[3];
+    compat_ih<COMPAT>(a, ih);
+    const int gd = d0 + (lane >> 3), gh = h0 + ((lane >> 1) & 3), gw = w0 + 2 * (lane & 1);
+    const float ev0 = float(gd), ev1 = float(gh), ev2 = float(gw);
+    float accR[2] = {0.f, 0.f}, accI[2] = {0.f, 0.f};
+    WarpStage4& S = stage[warp];
+    for (int base = rg.x; base < rg.y; base += 32) {
+        const int kept = stage4<COMPAT, false>(a, S, base, min(32, rg.y - base), lane, d0, h0, w0, ih);
+        __syncwarp();
+        for (int j = 0; j < kept; ++j) {
+            const Rec g = S.rec[j];
+            const float e0 = __fsub_rn(ev0, g.c0), e1 = __fsub_rn(ev1, g.c1);
+            const float e2a = __fsub_rn(ev2, g.c2), e2b = __fsub_rn(ev2 + 1.0f, g.c2);
+            const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
+            const float m0 = row_m(g.q22, A, B, e2a), m1 = row_m(g.q22, A, B, e2b);
+            if (!__any_sync(kFull, m0 <= kCut || m1 <= kCut)) continue;
+            if (m0 <= kCut) {
+                const float wgt = ex2_approx(m0 * kNegHalfLog2e);
+                accR[0] = fmaf(wgt, g.rho_r, accR[0]);
+                accI[0] = fmaf(wgt, g.rho_i, accI[0]);
+            }
+            if (m1 <= kCut) {
+                const float wgt = ex2_approx(m1 * kNegHalfLog2e);
+                accR[1] = fmaf(wgt, g.rho_r, accR[1]);
+                accI[1] = fmaf(wgt, g.rho_i, accI[1]);
+            }
+        }
+        __syncwarp();
+    }
+    if (gd >= a.d || gh >= a.h) return;
+    const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
+    if (PLANAR) {
+        for (int i = 0; i < 2; ++i)
+            if (gw + i < a.w) {
+                a.vol_r[flat + i] = accR[i];
+                a.vol_i[flat + i] = accI[i];
+            }
+    } else if (gw + 1 < a.w && (a.w & 1) == 0) {
+        reinterpret_cast<float4*>(a.vol)[flat >> 1] = make_float4(accR[0], accI[0], accR[1], accI[1]);
+    } else {
+        float2* out = reinterpret_cast<float2*>(a.vol) + flat;
+        for (int i = 0; i < 2; ++i)
+            if (gw + i < a.w) out[i] = make_float2(accR[i], accI[i]);
+    }
+}
+
+template <bool COMPAT, bool DET>
+__global__ void __launch_bounds__(kThreads) k_backward4(const RenderArgs a) {
+    __shared__ WarpStage4 stage[kWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t tile = int64_t(blockIdx.x) * kWarps + warp;
+    if (tile >= a.ntiles) return;  // warp-uniform; no CTA barrier below
+    const int2 rg = a.ranges[tile];
+    if (rg.x >= rg.y) return;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    float ih[3];
+    compat_ih<COMPAT>(a, ih);
+    const int gd = d0 + (lane >> 3), gh = h0 + ((lane >> 1) & 3), gw = w0 + 2 * (lane & 1);
+    float gr[2] = {0.f, 0.f}, gi[2] = {0.f, 0.f};
+    if (gd < a.d && gh < a.h) {
+        const int64_t flat = (int64_t(gd) * a.h + gh) * a.w + gw;
+        for (int i = 0; i < 2; ++i)
+            if (gw + i < a.w) {
+                if (COMPAT) {
+                    gr[i] = __ldg(a.gv_r + flat + i);
+                    gi[i] = __ldg(a.gv_i + flat + i);
+                } else {
+                    const float2 x = __ldg(reinterpret_cast<const float2*>(a.gvol) + flat + i);
+                    gr[i] = x.x;
+                    gi[i] = x.y;
+                }
+            }
+    }
+    const float ev0 = float(gd), ev1 = float(gh), ev2 = float(gw);
+    WarpStage4& S = stage[warp];
+    for (int base = rg.x; base < rg.y; base += 32) {
+        const int kept = stage4<COMPAT, DET>(a, S, base, min(32, rg.y - base), lane, d0, h0, w0, ih);
+        __syncwarp();
+        for (int j = 0; j < kept; ++j) {
+            const Rec g = S.rec[j];
+            const float e0 = __fsub_rn(ev0, g.c0), e1 = __fsub_rn(ev1, g.c1);
+            const float e2v[2] = {__fsub_rn(ev2, g.c2), __fsub_rn(ev2 + 1.0f, g.c2)};
+            const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
+            const float m[2] = {row_m(g.q22, A, B, e2v[0]), row_m(g.q22, A, B, e2v[1])};
+            if (!__any_sync(kFull, m[0] <= kCut || m[1] <= kCut)) {
+                if (DET && lane == 0) {  // no included voxel here: the pair's partial is zero
+                    float4* dst = reinterpret_cast<float4*>(a.partials + int64_t(S.pidx[j]) * kMomStride);
+                    dst[0] = dst[1] = dst[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                continue;
+            }
+            const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
+            float Dr = 0.f, Di = 0.f, R0 = 0.f, R1 = 0.f, R2 = 0.f;
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (m[k] <= kCut) {
+                    const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
+                    const float av = wgt * fmaf(hi, gi[k], hr * gr[k]);
+                    Dr = fmaf(wgt, gr[k], Dr);
+                    Di = fmaf(wgt, gi[k], Di);
+                    R0 += av;
+                    const float ae = av * e2v[k];
+                    R1 += ae;
+                    R2 = fmaf(ae, e2v[k], R2);
+                }
+            }
+            float v[16];
+            v[0] = Dr;
+            v[1] = Di;
+            v[2] = e0 * R0;
+            v[3] = e1 * R0;
+            v[4] = R1;
+            v[5] = (e0 * e0) * R0;
+            v[6] = e1 * v[2];
+            v[7] = e0 * R1;
+            v[8] = (e1 * e1) * R0;
+            v[9] = e1 * R1;
+            v[10] = R2;
+            const int gid = S.gid[j];
+            if (COMPAT) {
+#pragma unroll
+                for (int i = 11; i < 16; ++i) v[i] = 0.f;
+                compat_emit(a, g, gid, warp_reduce_scatter16(v, lane), lane, ih);
+            } else {
+                v[11] = 0.f;
+                const float tot = warp_reduce_scatter12(v, lane);
+                const int mi = moment12(lane);
+                if (!(lane & 1) && mi >= 0 && mi < kMom) {
+                    if (DET) a.partials[int64_t(S.pidx[j]) * kMomStride + mi] = tot;
+                    else atomicAdd(a.accum + int64_t(gid) * kMomStride + mi, tot);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Generic tile edge: one voxel per thread, Gaussians staged per CTA.
 // ---------------------------------------------------------------------------
 
@@ -1030,6 +1231,8 @@ int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void*
     }
     if (shape.tile_size == 8 && rpl == 2) k_forward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
     else if (shape.tile_size == 8) k_forward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
+    else if (shape.tile_size == 4)
+        k_forward4<false, false><<<unsigned((ntiles + kWarps - 1) / kWarps), kThreads, 0, st>>>(a);
     else k_forward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
@@ -1084,7 +1287,10 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
             else if (rpl == 2) k_backward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
             else k_backward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
         } else {
-            if (det) k_backward_generic<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+            const unsigned g4 = unsigned((ntiles + kWarps - 1) / kWarps);
+            if (shape.tile_size == 4 && det) k_backward4<false, true><<<g4, kThreads, 0, st>>>(a);
+            else if (shape.tile_size == 4) k_backward4<false, false><<<g4, kThreads, 0, st>>>(a);
+            else if (det) k_backward_generic<false, true><<<unsigned(ntiles), kThreads, 0, st>>>(a);
             else k_backward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
         }
         GSV_LAUNCH_CHECK();
@@ -1122,6 +1328,8 @@ int gsv_tile_forward(const float* centers, const float* cov_inv, const float* de
     a.vol_i = vol_i;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (tile_size == 8) k_forward8<true, true, 2><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    else if (tile_size == 4)
+        k_forward4<true, true><<<unsigned((num_tiles + kWarps - 1) / kWarps), kThreads, 0, st>>>(a);
     else k_forward_generic<true, true><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
@@ -1163,6 +1371,8 @@ int gsv_tile_backward(const float* centers, const float* cov_inv, const float* d
     a.g_dr = grad_den_r;
     a.g_di = grad_den_i;
     if (tile_size == 8) k_backward8<true, false, 2><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
+    else if (tile_size == 4)
+        k_backward4<true, false><<<unsigned((num_tiles + kWarps - 1) / kWarps), kThreads, 0, st>>>(a);
     else k_backward_generic<true, false><<<unsigned(num_tiles), kThreads, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
