@@ -127,11 +127,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units",
+// 2016): 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the SFU's
+// tanh.approx; its outputs are rounded to BF16, far coarser than the
+// approximation.
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC0 = 0.7978845608028654f;       // sqrt(2/pi)
+constexpr float kGeluC1 = 0.7978845608028654f * 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+    const float t = tanh_approx(x * fmaf(kGeluC1, x * x, kGeluC0));
+    return 0.5f * x * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
-    return cdf + x * pdf;
+    const float x2 = x * x;
+    const float t = tanh_approx(x * fmaf(kGeluC1, x2, kGeluC0));
+    const float du = fmaf(3.0f * kGeluC1, x2, kGeluC0);
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
@@ -239,7 +254,7 @@ __device__ __forceinline__ float bias_of(const GemmArgs& g, int n) {
 // of stage kt + STAGES - 1.  The epilogue moves the accumulator out of TMEM
 // 32 columns at a time and, for row-major outputs, transposes it through
 // shared memory so that lanes store consecutive columns (coalesced).
-template <int BN, int STAGES>
+template <int BN, int STAGES, int EPI>
 __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen05(const GemmArgs g) {
     constexpr int kATile = kBM * kBK * 2;   // 16 KB
     constexpr int kBTile = BN * kBK * 2;    // 32 KB for BN = 256
@@ -329,6 +344,7 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
         if (g.c_sn == 1) {
             float* scr = reinterpret_cast<float*>(smem) + warp * 32 * 33;
             const int col = lane % CW, rsub = lane / CW;
+            const int64_t step = int64_t(32 / CW) * g.c_sm;  // rows a lane advances per j
             for (int c0 = cbeg; c0 < cend; c0 += CW) {
                 float v[CW];
                 if constexpr (CW == 32) tmem_ld32(lane_addr + c0, v);
@@ -338,21 +354,22 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
                 __syncwarp();
                 const int n = n0 + c0 + col;
                 const bool n_ok = n < g.N;
-                if (g.epi == EPI_GELU_GRAD) {
+                const int64_t idx0 = int64_t(row0 + rsub) * g.c_sm + n;
+                if constexpr (EPI == EPI_GELU_GRAD) {
                     // all loads of the chunk in flight before the first use
                     float zv[CW];
 #pragma unroll
                     for (int j = 0; j < CW; ++j) {
                         const int row = row0 + j * (32 / CW) + rsub;
-                        zv[j] = (n_ok && row < g.M) ? g.z_f32[row * g.c_sm + n] : 0.f;
+                        zv[j] = (n_ok && row < g.M) ? g.z_f32[idx0 + j * step] : 0.f;
                     }
                     float cs = 0.f;
 #pragma unroll
                     for (int j = 0; j < CW; ++j) {
-                        const int r = j * (32 / CW) + rsub, row = row0 + r;
-                        if (n_ok && row < g.M) {
+                        const int r = j * (32 / CW) + rsub;
+                        if (n_ok && row0 + r < g.M) {
                             const __nv_bfloat16 o = __float2bfloat16(scr[r * 33 + col] * gelu_grad(zv[j]));
-                            g.out_bf16[row * g.c_sm + n] = o;
+                            g.out_bf16[idx0 + j * step] = o;
                             cs += __bfloat162float(o);
                         }
                     }
@@ -362,7 +379,17 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
 #pragma unroll 8
                     for (int j = 0; j < CW; ++j) {
                         const int r = j * (32 / CW) + rsub;
-                        if (n_ok && row0 + r < g.M) epi_store(g, row0 + r, n, scr[r * 33 + col], bn);
+                        if (!(n_ok && row0 + r < g.M)) continue;
+                        const int64_t ci = idx0 + j * step;
+                        const float x = scr[r * 33 + col];
+                        if constexpr (EPI == EPI_F32) {
+                            g.out_f32[ci] = x + bn;
+                        } else if constexpr (EPI == EPI_BIAS_GELU) {
+                            g.z_f32[ci] = x + bn;
+                            g.out_bf16[ci] = __float2bfloat16(gelu(x + bn));
+                        } else {
+                            atomicAdd(g.out_f32 + ci, x);
+                        }
                     }
                 }
                 __syncwarp();
@@ -385,6 +412,26 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+// Split-K weight gradients walk long K ranges: 4 stages hide the copy
+// latency there; the other products (K <= 256) keep 2 stages and 2 CTAs/SM.
+template <int EPI>
+int launch_gemm(const GemmArgs& g, int bn, dim3 grid, cudaStream_t st) {
+    constexpr int kStages = (EPI == EPI_ATOMIC_F32) ? 4 : 2;
+    if (bn == 256) {
+        const int smem = kStages * (kBM * kBK * 2 + 256 * kBK * 2);
+        GSV_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tcgen05<256, kStages, EPI>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_gemm_tcgen05<256, kStages, EPI><<<grid, kThreads, smem, st>>>(g);
+    } else {
+        const int smem = kStages * (kBM * kBK * 2 + 16 * kBK * 2);
+        GSV_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tcgen05<16, kStages, EPI>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_gemm_tcgen05<16, kStages, EPI><<<grid, kThreads, smem, st>>>(g);
+    }
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
 }
 
 // Operand copy mode: 16-byte cp.async needs a 16-byte aligned base and a
@@ -426,20 +473,14 @@ int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, l
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int bn = (N % 256 == 0) ? 256 : 16;
     dim3 grid((M + kBM - 1) / kBM, N / bn, zs);
-    constexpr int kStages = 2;
-    if (bn == 256) {
-        const int smem = kStages * (kBM * kBK * 2 + 256 * kBK * 2);
-        GSV_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tcgen05<256, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          smem));
-        k_gemm_tcgen05<256, kStages><<<grid, kThreads, smem, st>>>(g);
-    } else {
-        const int smem = kStages * (kBM * kBK * 2 + 16 * kBK * 2);
-        GSV_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tcgen05<16, kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          smem));
-        k_gemm_tcgen05<16, kStages><<<grid, kThreads, smem, st>>>(g);
+    int rc = GSV_OK;
+    switch (epi) {
+        case EPI_F32: rc = launch_gemm<EPI_F32>(g, bn, grid, st); break;
+        case EPI_BIAS_GELU: rc = launch_gemm<EPI_BIAS_GELU>(g, bn, grid, st); break;
+        case EPI_GELU_GRAD: rc = launch_gemm<EPI_GELU_GRAD>(g, bn, grid, st); break;
+        default: rc = launch_gemm<EPI_ATOMIC_F32>(g, bn, grid, st); break;
     }
-    GSV_LAUNCH_CHECK();
-    return GSV_OK;
+    return rc;
 }
 
 }  // extern "C"

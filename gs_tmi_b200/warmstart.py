@@ -6,7 +6,7 @@ seed's intensity-seeded scale; padded to 256) to the initial parameters of
 the Gaussian at that seed: centre offset (3), log-scale (3), quaternion (4)
 and complex density (2); padded to 16 outputs.
 
-Network 256 -> 256 (GELU) -> 256 (GELU) -> 16 with BF16 weights and FP32
+Network 256 -> 256 (GELU, tanh form) -> 256 (GELU) -> 16 with BF16 weights and FP32
 accumulation.  Every matrix product of inference and training -- X W^T with
 the bias + GELU epilogue, dY W with the GELU' epilogue, and the split-K
 weight gradients dZ^T X -- runs on the hand-written tcgen05 kernel

@@ -26,8 +26,10 @@ def _cpu_reference(mlp, x, dout):
     W = [bf(w.detach().cpu()) for w in mlp.params[:3]]
     b = [p.detach().cpu().double() for p in mlp.params[3:]]
     xc = bf(x.cpu())
-    g = lambda z: 0.5 * z * (1 + torch.erf(z / math.sqrt(2)))
-    gp = lambda z: 0.5 * (1 + torch.erf(z / math.sqrt(2))) + z * torch.exp(-0.5 * z * z) / math.sqrt(2 * math.pi)
+    c0, c1 = math.sqrt(2 / math.pi), math.sqrt(2 / math.pi) * 0.044715  # GELU, tanh form
+    g = lambda z: 0.5 * z * (1 + torch.tanh(z * (c0 + c1 * z * z)))
+    gp = lambda z: (0.5 * (1 + torch.tanh(z * (c0 + c1 * z * z)))
+                    + 0.5 * z * (1 - torch.tanh(z * (c0 + c1 * z * z)) ** 2) * (c0 + 3 * c1 * z * z))
     z1 = xc @ W[0].t() + b[0]
     y1 = bf(g(z1))
     z2 = y1 @ W[1].t() + b[1]
