@@ -991,10 +991,13 @@ __device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
 #pragma unroll
     for (int i = 0; i < kMom; ++i) mo[i] = a.accum[g * kMomStride + i];
     const Rec R = a.recs[g];
-    // dL/dcenter_vox, then dcenter/dpositions = 0.5 * shape = hs   (:284)
-    const float dc0 = -(2.0f * R.q00 * mo[2] + R.q01x2 * mo[3] + R.q02x2 * mo[4]);
-    const float dc1 = -(R.q01x2 * mo[2] + 2.0f * R.q11 * mo[3] + R.q12x2 * mo[4]);
-    const float dc2 = -(R.q02x2 * mo[2] + R.q12x2 * mo[3] + 2.0f * R.q22 * mo[4]);
+    // dL/dcenter_vox, then dcenter/dpositions = 0.5 * shape = hs   (:284).
+    // The reference sums this over included pairs only: a Gaussian with none
+    // (e.g. NaN coefficients) gets exactly 0, not 0 * NaN.
+    const bool has_center = mo[2] != 0.f || mo[3] != 0.f || mo[4] != 0.f;
+    const float dc0 = has_center ? -(2.0f * R.q00 * mo[2] + R.q01x2 * mo[3] + R.q02x2 * mo[4]) : 0.f;
+    const float dc1 = has_center ? -(R.q01x2 * mo[2] + 2.0f * R.q11 * mo[3] + R.q12x2 * mo[4]) : 0.f;
+    const float dc2 = has_center ? -(R.q02x2 * mo[2] + R.q12x2 * mo[3] + 2.0f * R.q22 * mo[4]) : 0.f;
     out.positions[g * 3 + 0] = dc0 * a.hs[0];
     out.positions[g * 3 + 1] = dc1 * a.hs[1];
     out.positions[g * 3 + 2] = dc2 * a.hs[2];
