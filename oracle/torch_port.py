@@ -1,5 +1,6 @@
-"""PyTorch-CPU port of the reference's own CPU voxelizer path -- TEST / BASELINE
-INFRASTRUCTURE (bench.py's CPU-baseline leg and its ``--impl reference`` arm).
+"""PyTorch-CPU port of the reference's own CPU voxelizer path -- test and
+measurement infrastructure (bench.py's CPU-baseline leg and its
+``--impl reference`` arm).
 
 It restates, in FP32 torch on the host cores, what the reference runs when
 its CUDA extension is unavailable (3DGS/3dgsVC/gaussian/tile_voxelizer.py):
