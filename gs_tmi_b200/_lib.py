@@ -89,6 +89,7 @@ SIGNATURES = {
     "gsv_sense_residual": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _sz, _vp]),
     "gsv_sense_adjoint": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "gsv_tv_magnitude": (ctypes.c_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _sz, _vp]),
+    "gsv_knn3_mean_distance": (ctypes.c_int, [_vp, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),
 }

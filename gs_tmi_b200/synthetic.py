@@ -241,15 +241,21 @@ def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise
 
 
 def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float = 0.2,
-                    seed: int = 0) -> GaussianSet:
+                    seed: int = 0, device=None) -> GaussianSet:
     """Intensity-seeded initialisation in the manner of the reference's
     GaussianModel3D.from_image (gaussian_model.py:308-355, random mode):
     random voxel centres, isotropic scale = mean distance to the 3 nearest
     other centres (normalised units), identity rotation, density =
-    k * zero-filled value at the centre."""
+    k * zero-filled value at the centre.
+
+    `device` (a CUDA device): the 3-NN distances come from the library's
+    exact grid search (gsv_knn3_mean_distance) instead of scipy's cKDTree and
+    the set is returned on that device; the seed voxels are the same."""
+    d, h, w = image.shape
+    if device is not None and torch.device(device).type == "cuda":
+        return _from_image_init_gpu(image, num_points, density_scale_k, seed, torch.device(device))
     from scipy.spatial import cKDTree
 
-    d, h, w = image.shape
     total = d * h * w
     g = torch.Generator().manual_seed(seed)
     n = min(num_points, total)
@@ -267,6 +273,8 @@ def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float
         nd = torch.from_numpy(dist[:, 1:].astype("float32"))
         if nd.ndim == 1:
             nd = nd[:, None]
+        if nd.shape[1] < 3:  # fewer than 3 other seeds: the last distance repeats (:297-299)
+            nd = torch.cat([nd, nd[:, -1:].repeat(1, 3 - nd.shape[1])], 1)
         mean = nd[:, :3].mean(1, keepdim=True).clamp_min(1e-6)
     else:
         mean = torch.full((n, 1), 1e-3)
@@ -275,4 +283,37 @@ def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float
     rot[:, 0] = 1.0
     flat = image.reshape(-1)[idx]
     return GaussianSet(pos.float(), scales.float(), rot, (flat.real * density_scale_k).float(),
+                       (flat.imag * density_scale_k).float())
+
+
+def _from_image_init_gpu(image, num_points, density_scale_k, seed, dev) -> GaussianSet:
+    import ctypes
+
+    from ._lib import check, lib
+
+    d, h, w = image.shape
+    total = d * h * w
+    g = torch.Generator().manual_seed(seed)
+    n = min(num_points, total)
+    idx_cpu = torch.randperm(total, generator=g)[:n]
+    z = idx_cpu // (h * w)
+    rem = idx_cpu % (h * w)
+    y = rem // w
+    x = rem % w
+    # positions exactly as the CPU path rounds them
+    pos = torch.stack([((z.float() + 0.5) / d) * 2 - 1, ((y.float() + 0.5) / h) * 2 - 1,
+                       ((x.float() + 0.5) / w) * 2 - 1], -1).to(dev).contiguous()
+    idx = idx_cpu.to(dev)
+    mean = torch.empty(n, dtype=torch.float32, device=dev)
+    grid = torch.empty(total, dtype=torch.int32, device=dev)
+    check(lib.gsv_knn3_mean_distance(ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(pos.data_ptr()), n, d, h, w,
+                                     ctypes.c_void_p(grid.data_ptr()),
+                                     ctypes.c_void_p(mean.data_ptr()),
+                                     ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+          "gsv_knn3_mean_distance")
+    scales = mean[:, None].repeat(1, 3)
+    rot = torch.zeros(n, 4, device=dev)
+    rot[:, 0] = 1.0
+    flat = image.to(dev).reshape(-1)[idx]
+    return GaussianSet(pos.float().contiguous(), scales.contiguous(), rot, (flat.real * density_scale_k).float(),
                        (flat.imag * density_scale_k).float())

@@ -228,7 +228,7 @@ class TrainingCase:
 
 def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device):
     dev = torch.device(device)
-    base = synthetic.from_image_init(case.zero_filled, num_points, seed=seed).to(dev)
+    base = synthetic.from_image_init(case.zero_filled, num_points, seed=seed, device=dev).to(dev)
     shape = tuple(case.ground_truth.shape)
     zf = case.zero_filled.to(dev)
     scale = image_scale(zf)

@@ -286,6 +286,19 @@ GSV_API int gsv_sense_adjoint(const float* kgrad_image, const float* coils, int3
 GSV_API int gsv_tv_magnitude(const float* volume, int32_t d, int32_t h, int32_t w, float* loss, float* grad, void* ws,
                              size_t ws_bytes, void* stream);
 
+/* ---- intensity-seeded initialisation -------------------------------- */
+
+/* V/gaussian/gaussian_model.py:283-306 (_sampled_3nn_scale_init, a cKDTree on
+ * the CPU): for n distinct seed voxels (flat row-major indices into the
+ * (d,h,w) volume) with their FP32 normalised positions [n,3]
+ * ((v + 0.5) / shape * 2 - 1 per axis), mean_distance[i] = FP32 mean of the
+ * distances (FP64, rounded to FP32) from seed i to its 3 nearest other seeds,
+ * at least 1e-6; the last found distance repeats when fewer than 3 other seeds
+ * exist and a lone seed gets 1e-3.  grid: d*h*w int32 of device scratch.
+ * Exact (grid shells, no approximation). */
+GSV_API int gsv_knn3_mean_distance(const int64_t* voxels, const float* positions, int64_t n, int32_t d, int32_t h,
+                                   int32_t w, int32_t* grid, float* mean_distance, void* stream);
+
 /* ---- reference-compatible kernels (the pybind forward/backward) ------- */
 
 /* centers [n,3] voxel units, cov_inv [n,3,3] normalised units (symmetric;
