@@ -49,6 +49,25 @@ class GsvBatchItem(ctypes.Structure):
                 ("grad_volume", ctypes.c_void_p), ("grads", GsvGrads), ("chunk", ctypes.c_int32)]
 
 
+GSV_DENSITY_SPLIT = 0x1
+GSV_DENSITY_CLONE = 0x2
+GSV_DENSITY_PRUNE = 0x4
+GSV_DENSITY_ROW_OVERFLOW = 0x8
+
+
+class GsvDensityRows(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("log_scales", ctypes.c_void_p), ("rotations", ctypes.c_void_p),
+                ("density_r", ctypes.c_void_p), ("density_i", ctypes.c_void_p),
+                ("exp_avg", ctypes.c_void_p * 5), ("exp_avg_sq", ctypes.c_void_p * 5), ("capacity", ctypes.c_int64)]
+
+
+class GsvDensityConfig(ctypes.Structure):
+    _fields_ = [("grad_threshold", ctypes.c_float), ("scale_threshold", ctypes.c_float),
+                ("opacity_threshold", ctypes.c_float), ("max_scale", ctypes.c_float),
+                ("long_axis_offset_factor", ctypes.c_float), ("long_axis_split", ctypes.c_int32),
+                ("use_cloning", ctypes.c_int32), ("min_keep", ctypes.c_int32), ("max_points", ctypes.c_int64)]
+
+
 class GsvTuning(ctypes.Structure):
     _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
@@ -66,6 +85,7 @@ SIGNATURES = {
     "gsv_gauss_workspace_bytes": (_sz, [_i64, _S]),
     "gsv_pair_workspace_bytes": (_sz, [_i64, _S, ctypes.c_int]),
     "gsv_prepare": (ctypes.c_int, [_P, _S, _vp, _sz, _i64p, _vp]),
+    "gsv_prepare_live": (ctypes.c_int, [_P, _vp, _S, _vp, _sz, _i64p, _vp]),
     "gsv_bin": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp]),
     "gsv_bin_views": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsv_status_views": (ctypes.c_int, [_S, _i64, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
@@ -89,6 +109,10 @@ SIGNATURES = {
     "gsv_sense_residual": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _sz, _vp]),
     "gsv_sense_adjoint": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "gsv_tv_magnitude": (ctypes.c_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _sz, _vp]),
+    "gsv_density_workspace_bytes": (_sz, [_i64]),
+    "gsv_density_control": (ctypes.c_int, [ctypes.POINTER(GsvDensityRows), _vp, _vp,
+                                           ctypes.POINTER(GsvDensityConfig), _vp, _vp, _vp, _sz, _vp]),
+    "gsv_normal_fill": (ctypes.c_int, [_vp, _i64, ctypes.c_uint64, _vp, _vp]),
     "gsv_knn3_mean_distance": (ctypes.c_int, [_vp, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),

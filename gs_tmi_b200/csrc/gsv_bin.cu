@@ -158,13 +158,21 @@ __global__ void __launch_bounds__(256) k_prepare(const float* __restrict__ pos,
                                                  const float* __restrict__ scl,
                                                  const float* __restrict__ rot,
                                                  const float* __restrict__ dr,
-                                                 const float* __restrict__ di, int64_t n, DevShape s,
+                                                 const float* __restrict__ di, int64_t n,
+                                                 const int32_t* __restrict__ live, DevShape s,
                                                  Rec* __restrict__ recs, float4* __restrict__ ext,
                                                  int4* __restrict__ boxes,
                                                  int64_t* __restrict__ counts, Status* status) {
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g == 0) counts[n] = 0;
     if (g >= n) return;
+    if (live && g >= int64_t(*live)) {  // parked row: no tiles, no contribution
+        recs[g] = Rec{};
+        ext[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        boxes[g] = make_int4(0, 0, 0, 0);
+        counts[g] = 0;
+        return;
+    }
     float p[3], sc[3], q[4];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -387,8 +395,8 @@ size_t gsv_pair_workspace_bytes(int64_t capacity, gsv_shape shape, int flags) {
     return pair_layout(capacity, si, flags).total;
 }
 
-int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
-                int64_t* total_pairs_host, void* stream) {
+static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shape, void* ws_gauss,
+                        size_t ws_gauss_bytes, int64_t* total_pairs_host, void* stream) {
     ShapeInfo si = shape_info(shape);
     if (!si.ok || !p || p->n < 0 || p->n >= int64_t(INT32_MAX) || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
     const int64_t n = p->n;
@@ -400,7 +408,7 @@ int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_
     Status* status = at<Status>(ws_gauss, L.status);
     GSV_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(Status), st));
     k_prepare<<<grid_for(n + 1, 256), 256, 0, st>>>(p->positions, p->scales, p->rotations, p->density_r,
-                                                    p->density_i, n, dev_shape(si), at<Rec>(ws_gauss, L.rec),
+                                                    p->density_i, n, live, dev_shape(si), at<Rec>(ws_gauss, L.rec),
                                                     at<float4>(ws_gauss, L.ext),
                                                     at<int4>(ws_gauss, L.box), at<int64_t>(ws_gauss, L.counts),
                                                     status);
@@ -411,6 +419,17 @@ int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_
                                                at<int64_t>(ws_gauss, L.offsets), int(n + 1), st));
     if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
     return GSV_OK;
+}
+
+int gsv_prepare(const gsv_params* p, gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
+                int64_t* total_pairs_host, void* stream) {
+    return prepare_impl(p, nullptr, shape, ws_gauss, ws_gauss_bytes, total_pairs_host, stream);
+}
+
+int gsv_prepare_live(const gsv_params* p, const int32_t* live, gsv_shape shape, void* ws_gauss,
+                     size_t ws_gauss_bytes, int64_t* total_pairs_host, void* stream) {
+    if (!live) return GSV_ERR_INVALID_ARGUMENT;
+    return prepare_impl(p, live, shape, ws_gauss, ws_gauss_bytes, total_pairs_host, stream);
 }
 
 int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,

@@ -55,6 +55,8 @@ class FitConfig:
     max_scale: float = 0.5
     max_points: int = 500_000
     use_cloning: bool = True
+    long_axis_split: bool = False        # "long_axis" strategy: deterministic children (gaussian_model.py:112-131)
+    long_axis_offset_factor: float = 1.0
     tile_size: int = 8
     deterministic: bool = False
     eval_every: int = 100
@@ -261,12 +263,24 @@ def transplant(old_opt, new_opt, keep: torch.Tensor, n_new: int):
         new_opt.state[np_] = new_state
 
 
+def _quat_rotation(q: torch.Tensor) -> torch.Tensor:
+    """quaternion_to_rotation_matrix (gaussian_model.py:12-19)."""
+    q = q / (q.norm(dim=-1, keepdim=True) + 1e-8)
+    w, x, y, z = q.unbind(-1)
+    return torch.stack([torch.stack([1 - 2 * y * y - 2 * z * z, 2 * x * y - 2 * z * w, 2 * x * z + 2 * y * w], -1),
+                        torch.stack([2 * x * y + 2 * z * w, 1 - 2 * x * x - 2 * z * z, 2 * y * z - 2 * x * w], -1),
+                        torch.stack([2 * x * z - 2 * y * w, 2 * y * z + 2 * x * w, 1 - 2 * x * x - 2 * y * y], -1)],
+                       -2)
+
+
 @torch.no_grad()
-def density_control(p: GaussianParams, pos_grad: torch.Tensor, cfg: FitConfig, gen: torch.Generator,
-                    on_event: Callable[[torch.Tensor], None]):
+def density_control(p: GaussianParams, pos_grad: torch.Tensor, cfg: FitConfig, gen: Optional[torch.Generator],
+                    on_event: Callable[[torch.Tensor], None], noise: Optional[torch.Tensor] = None):
     """Split, clone, prune (trainer.py:294-352, gaussian_model.py:85-186).
     After every change of the parameter tensors ``on_event(keep_mask)`` runs
-    (the optimiser rebuild of trainer.py:391-424); returns the event count."""
+    (the optimiser rebuild of trainer.py:391-424); returns the event count.
+    ``noise`` [N,6]: the standard normals of the two children of each row
+    (columns 0-2 and 3-5) instead of draws from ``gen``."""
     events = 0
     if p.n >= cfg.max_points:
         return events
@@ -281,14 +295,36 @@ def density_control(p: GaussianParams, pos_grad: torch.Tensor, cfg: FitConfig, g
         did_split_branch = True
         par_pos = p.positions[split]
         par_s = scales[split]
-        na = torch.randn(par_pos.shape, device=par_pos.device, generator=gen) * par_s * 0.5
-        nb = torch.randn(par_pos.shape, device=par_pos.device, generator=gen) * par_s * 0.5
         keep = ~split
-        new = [torch.cat([p.positions[keep], par_pos + na, par_pos + nb]),
-               torch.cat([p.log_scales[keep], torch.log(par_s / 1.6 + 1e-8).repeat(2, 1)]),
+        if cfg.long_axis_split:
+            # gaussian_model.py:112-131
+            axis = par_s.argmax(dim=-1)
+            rows = torch.arange(n_split, device=par_s.device)
+            child = par_s.clone()
+            child[rows, axis] *= 0.5
+            other = torch.ones_like(child, dtype=torch.bool)
+            other[rows, axis] = False
+            child[other] *= 0.85
+            local = torch.zeros_like(par_pos)
+            local[rows, axis] = child[rows, axis] * cfg.long_axis_offset_factor
+            shift = torch.bmm(_quat_rotation(p.rotations[split]), local.unsqueeze(-1)).squeeze(-1)
+            pos_new = [par_pos + shift, par_pos - shift]
+            ls_new = torch.log(child + 1e-8).repeat(2, 1)
+            dfac = 0.6
+        else:
+            if noise is not None:
+                za, zb = noise[split, :3], noise[split, 3:]
+            else:
+                za = torch.randn(par_pos.shape, device=par_pos.device, generator=gen)
+                zb = torch.randn(par_pos.shape, device=par_pos.device, generator=gen)
+            pos_new = [par_pos + za * par_s * 0.5, par_pos + zb * par_s * 0.5]
+            ls_new = torch.log(par_s / 1.6 + 1e-8).repeat(2, 1)
+            dfac = 0.5
+        new = [torch.cat([p.positions[keep], *pos_new]),
+               torch.cat([p.log_scales[keep], ls_new]),
                torch.cat([p.rotations[keep], p.rotations[split].repeat(2, 1)]),
-               torch.cat([p.density_r[keep], (p.density_r[split] * 0.5).repeat(2)]),
-               torch.cat([p.density_i[keep], (p.density_i[split] * 0.5).repeat(2)])]
+               torch.cat([p.density_r[keep], (p.density_r[split] * dfac).repeat(2)]),
+               torch.cat([p.density_i[keep], (p.density_i[split] * dfac).repeat(2)])]
         p.replace(new)
         on_event(keep)
         events += 1
@@ -310,7 +346,7 @@ def density_control(p: GaussianParams, pos_grad: torch.Tensor, cfg: FitConfig, g
             events += 1
     scales = torch.exp(p.log_scales)
     smax = scales.max(-1)[0]
-    mag = torch.sqrt(p.density_r * p.density_r + p.density_i * p.density_i)
+    mag = torch.abs(torch.complex(p.density_r, p.density_i))
     prune = (mag < cfg.opacity_threshold) | (smax > cfg.max_scale)
     keep = ~prune
     if int(keep.sum()) >= 100 and int(prune.sum()) > 0:
@@ -340,10 +376,12 @@ class FitResult:
 
 def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Callable] = None,
         device="cuda:0", stop_nmse: Optional[float] = None, log: Optional[Callable] = None,
-        eval_ssim: bool = True) -> FitResult:
+        eval_ssim: bool = True, split_noise: Optional[Callable[[int], torch.Tensor]] = None) -> FitResult:
     """Plain 3DGSMR fit of `case` from `init`.  Wall time excludes the
     evaluations; `stop_nmse` ends the fit at the first evaluation at or below
-    that hard-DC NMSE (time-to-NMSE runs)."""
+    that hard-DC NMSE (time-to-NMSE runs).  `split_noise(n)`, called once
+    per densifying iteration, gives the [n,6] split noise instead of draws
+    from the fit's generator."""
     dev = torch.device(device)
     shape = tuple(case.ground_truth.shape)
     if voxelizer is None:
@@ -392,7 +430,8 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
                 transplant(holder[0], new_opt, keep, p.n)
                 holder[0] = new_opt
 
-            if density_control(p, pos_grad, cfg, gen, rebuild):
+            noise = split_noise(p.n) if split_noise is not None else None
+            if density_control(p, pos_grad, cfg, gen, rebuild, noise=noise):
                 opt = holder[0]
                 skip_sched = True
         if skip_sched:

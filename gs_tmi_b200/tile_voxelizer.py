@@ -180,9 +180,15 @@ class StaticPlan(BinPlan):
     beyond the capacity are dropped and GSV_FLAG_CAPACITY_OVERFLOW is latched
     in ``flags_dev`` (copy it out and check it after each replay)."""
 
-    def __init__(self, shape: GsvShape, n: int, device: torch.device, capacity: int, flags: int = 0):
+    def __init__(self, shape: GsvShape, n: int, device: torch.device, capacity: int, flags: int = 0,
+                 live: Optional[torch.Tensor] = None):
         super().__init__(shape, n, device, flags)
         self.alloc_pairs(capacity)
+        # live: device int32 [1]; only the first live[0] of the n rows are
+        # Gaussians (rows managed by gsv_density_control)
+        if live is not None and (live.dtype != torch.int32 or not live.is_cuda or live.numel() != 1):
+            raise ValueError("live must be a one-element int32 tensor on the plan's device")
+        self.live = live
         fl, tot = ctypes.c_void_p(), ctypes.c_void_p()
         check(lib.gsv_status_views(shape, n, _ptr(self.ws_gauss), ctypes.byref(fl), ctypes.byref(tot)),
               "gsv_status_views")
@@ -203,8 +209,12 @@ class _VoxelizeStaticFn(torch.autograd.Function):
             raise ValueError(f"static plan is sized for {plan.n} Gaussians, got {int(params[0].shape[0])}")
         st = _stream(dev)
         gp = GsvParams(*(t.data_ptr() for t in params), plan.n)
-        check(lib.gsv_prepare(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), plan.gauss_bytes, None, st),
-              "gsv_prepare")
+        if plan.live is None:
+            check(lib.gsv_prepare(ctypes.byref(gp), plan.shape, _ptr(plan.ws_gauss), plan.gauss_bytes, None, st),
+                  "gsv_prepare")
+        else:
+            check(lib.gsv_prepare_live(ctypes.byref(gp), _ptr(plan.live), plan.shape, _ptr(plan.ws_gauss),
+                                       plan.gauss_bytes, None, st), "gsv_prepare_live")
         check(lib.gsv_bin(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.pair_bytes,
                           plan.capacity, st), "gsv_bin")
         vol = torch.empty((plan.shape.d, plan.shape.h, plan.shape.w), dtype=torch.complex64, device=dev)
@@ -351,12 +361,13 @@ class TileVoxelizer(nn.Module):
             dr, di = density, torch.zeros_like(density)
         return _VoxelizeFn.apply(positions, scales, rotations, dr, di, self._shape, self.deterministic, self.tuner)
 
-    def static(self, n: int, capacity: int) -> "StaticVoxelizer":
+    def static(self, n: int, capacity: int, live: Optional[torch.Tensor] = None) -> "StaticVoxelizer":
         """A sync-free, allocation-free variant for `n` Gaussians and at most
-        `capacity` (tile, Gaussian) pairs, for CUDA-graph capture."""
+        `capacity` (tile, Gaussian) pairs, for CUDA-graph capture.  With
+        `live` (device int32 [1]) only the first live[0] rows are Gaussians."""
         flags = _lib.GSV_BACKWARD_DETERMINISTIC if self.deterministic else 0
         dev = torch.device(self.device) if not isinstance(self.device, torch.device) else self.device
-        return StaticVoxelizer(StaticPlan(self._shape, int(n), dev, int(capacity), flags))
+        return StaticVoxelizer(StaticPlan(self._shape, int(n), dev, int(capacity), flags, live=live))
 
     def count_pairs(self, positions: torch.Tensor, scales: torch.Tensor) -> int:
         """Pair total of the current parameters (one host sync)."""

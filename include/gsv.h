@@ -119,6 +119,13 @@ GSV_API size_t gsv_pair_workspace_bytes(int64_t capacity, gsv_shape shape, int f
 GSV_API int gsv_prepare(const gsv_params* params, gsv_shape shape, void* ws_gauss, size_t ws_gauss_bytes,
                 int64_t* total_pairs_host, void* stream);
 
+/* gsv_prepare over capacity-sized parameter rows of which only the first
+ * `*live` (a device int32, read on the stream) are Gaussians: the other rows
+ * get no tiles and contribute nothing, and their gradients are zero.  Used
+ * with gsv_density_control, which changes the live count on the device. */
+GSV_API int gsv_prepare_live(const gsv_params* params, const int32_t* live, gsv_shape shape, void* ws_gauss,
+                             size_t ws_gauss_bytes, int64_t* total_pairs_host, void* stream);
+
 /* Emit (tile, Gaussian) pairs, radix-sort them by tile (stable: ascending
  * Gaussian id within a tile) and build the per-tile ranges.  If the pair
  * total exceeds `capacity` only `capacity` pairs are kept and
@@ -287,6 +294,60 @@ GSV_API int gsv_tv_magnitude(const float* volume, int32_t d, int32_t h, int32_t 
                              size_t ws_bytes, void* stream);
 
 /* ---- intensity-seeded initialisation -------------------------------- */
+
+/* ---- adaptive density control on the device ---------------------------- */
+
+/* trainer.py:294-424 (adaptive_density_control, _transplant_adam_state,
+ * _rebuild_optimizer) with gaussian_model.py:85-222 (densify_and_split,
+ * densify_and_clone, _update_params), applied in place to capacity-sized rows
+ * whose live count is a device word, with no host synchronisation (CUDA-graph
+ * capturable).  Rows past the live count are parked: zero moments, unit
+ * scale, identity rotation, zero density; gsv_prepare_live skips them. */
+typedef struct gsv_density_rows { /* device pointers, FP32, row-major [capacity, width] */
+    float* positions;     /* width 3 */
+    float* log_scales;    /* width 3 */
+    float* rotations;     /* width 4 */
+    float* density_r;     /* width 1 */
+    float* density_i;     /* width 1 */
+    float* exp_avg[5];    /* Adam first moments of the five tensors above, or all NULL */
+    float* exp_avg_sq[5]; /* Adam second moments, or all NULL */
+    int64_t capacity;
+} gsv_density_rows;
+
+typedef struct gsv_density_config {
+    float grad_threshold;          /* |dL/dposition| > this: densify candidate */
+    float scale_threshold;         /* max scale > this: split, else clone */
+    float opacity_threshold;       /* |density| < this: prune */
+    float max_scale;               /* max scale > this: prune */
+    float long_axis_offset_factor; /* long-axis children shift (gaussian_model.py:119-131) */
+    int32_t long_axis_split;       /* 1: long-axis children; 0: N(parent, (s/2)^2) children from `noise` */
+    int32_t use_cloning;           /* clone branch enabled */
+    int32_t min_keep;              /* prune only when at least this many rows survive (100) */
+    int64_t max_points;            /* no densification at or beyond this many rows */
+} gsv_density_config;
+
+/* report[0] bits; report[1..3] = rows split, cloned, pruned. */
+#define GSV_DENSITY_SPLIT 0x1
+#define GSV_DENSITY_CLONE 0x2
+#define GSV_DENSITY_PRUNE 0x4
+#define GSV_DENSITY_ROW_OVERFLOW 0x8 /* the branch needs more rows than `capacity`: nothing was changed */
+
+GSV_API size_t gsv_density_workspace_bytes(int64_t capacity);
+/* One density-control step.  pos_grad [capacity,3]: the position gradient
+ * before clipping; noise [capacity,6]: standard normals for the two children
+ * of a split parent row (first child columns 0-2, second 3-5), unused with
+ * long_axis_split; live: device int32, read and updated; report: device
+ * int32[4], written. */
+GSV_API int gsv_density_control(const gsv_density_rows* rows, const float* pos_grad, const float* noise,
+                                const gsv_density_config* cfg, int32_t* live, int32_t* report, void* ws,
+                                size_t ws_bytes, void* stream);
+
+/* `count` standard normals (Philox4x32-10 with Box-Muller) of stream
+ * `*counter` (a device int64, read on the stream) under key `seed`, then
+ * *counter += 1: a graph replay draws a fresh stream, and restoring the
+ * counter replays the same draws.  The split noise of gsv_density_control
+ * (torch.randn_like at gaussian_model.py:135-136). */
+GSV_API int gsv_normal_fill(float* out, int64_t count, uint64_t seed, int64_t* counter, void* stream);
 
 /* V/gaussian/gaussian_model.py:283-306 (_sampled_3nn_scale_init, a cKDTree on
  * the CPU): for n distinct seed voxels (flat row-major indices into the

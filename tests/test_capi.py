@@ -101,3 +101,48 @@ def test_no_cpu_fallback():
             gs_tmi_b200.TileVoxelizer((8, 8, 8))
         with pytest.raises(ValueError):
             gs_tmi_b200.build_tile_pairs(torch.zeros(2, 3), torch.ones(2), (8, 8, 8), 8)
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every struct of include/gsv.h has the size and field offsets its
+    ctypes mirror assumes (gcc compiles a probe against the header)."""
+    import ctypes
+    import shutil
+
+    from gs_tmi_b200 import _lib
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    mirrors = {"gsv_shape": _lib.GsvShape, "gsv_params": _lib.GsvParams, "gsv_grads": _lib.GsvGrads,
+               "gsv_batch_item": _lib.GsvBatchItem, "gsv_tuning": _lib.GsvTuning,
+               "gsv_density_rows": _lib.GsvDensityRows, "gsv_density_config": _lib.GsvDensityConfig}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "gsv.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, cls in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_density_host_queries():
+    from gs_tmi_b200 import density
+    from gs_tmi_b200._lib import GSV_ERR_INVALID_ARGUMENT, lib
+
+    assert lib.gsv_density_workspace_bytes(0) == 0
+    assert lib.gsv_density_workspace_bytes(100_000) >= 100_000 * (36 * 4 + 16)
+    assert lib.gsv_density_control(None, None, None, None, None, None, None, 0, None) == GSV_ERR_INVALID_ARGUMENT
+    assert lib.gsv_normal_fill(None, 4, 0, None, None) == GSV_ERR_INVALID_ARGUMENT
+    assert density.initial_rows(50_000, 500_000) == 100_352
+    assert density.initial_rows(1000, 500_000) == 65_536
+    assert density.initial_rows(400_000, 500_000) == 500_000
+    assert density.initial_rows(600_000, 500_000) == 600_000

@@ -81,3 +81,61 @@ def test_metrics():
                        data_range=L)
     assert abs(one - s) < 1e-10
     del xa, yb
+
+
+def _params(pos, scales, rot, dr, di):
+    return sense.GaussianParams(synthetic.GaussianSet(torch.tensor(pos), torch.tensor(scales), torch.tensor(rot),
+                                                      torch.tensor(dr), torch.tensor(di)), "cpu")
+
+
+def test_long_axis_split_on_cpu():
+    """gaussian_model.py:112-131: the longest axis halves, the others shrink
+    by 0.85, the children sit at +/- child_scale along the rotated axis,
+    densities x0.6; the survivors come first."""
+    p = _params([[0.1, 0.2, 0.3], [0.0, 0.0, 0.0]], [[0.02, 0.05, 0.03], [0.02, 0.02, 0.02]],
+                [[1.0, 0.0, 0.0, 0.0], [1.0, 0.0, 0.0, 0.0]], [1.0, 2.0], [0.5, 1.0])
+    cfg = sense.FitConfig(long_axis_split=True, use_cloning=False, grad_threshold=0.01, scale_threshold=0.03,
+                          opacity_threshold=0.01, max_points=100)
+    grad = torch.tensor([[0.02, 0.0, 0.0], [0.02, 0.0, 0.0]])
+    events = sense.density_control(p, grad, cfg, None, lambda keep: None)
+    assert events == 1 and p.n == 3
+    assert torch.equal(p.positions[0], torch.tensor([0.0, 0.0, 0.0]))  # the survivor
+    child = torch.tensor([0.02 * 0.85, 0.05 * 0.5, 0.03 * 0.85])
+    for row, sign in ((1, 1.0), (2, -1.0)):
+        assert torch.allclose(p.positions[row], torch.tensor([0.1, 0.2 + sign * 0.025, 0.3]), atol=1e-7)
+        assert torch.allclose(torch.exp(p.log_scales[row]), child, rtol=1e-6)
+        assert torch.allclose(p.density_r[row], torch.tensor(0.6)) and torch.allclose(p.density_i[row],
+                                                                                      torch.tensor(0.3))
+
+
+def test_split_noise_and_prune_on_cpu():
+    """Children at parent + z * s / 2 with the given noise, scales s / 1.6;
+    |rho| below the opacity threshold is pruned (complex magnitude)."""
+    n = 120
+    g = torch.Generator().manual_seed(0)
+    pos = (torch.rand(n, 3, generator=g) * 2 - 1)
+    scales = torch.full((n, 3), 0.005)
+    scales[0] = 0.05                                   # the one split parent
+    rot = torch.zeros(n, 4)
+    rot[:, 0] = 1.0
+    dr = torch.full((n,), 0.5)
+    di = torch.zeros(n)
+    dr[5], di[5] = 0.006, 0.008                         # |rho| = 0.01: kept (not < 0.01)
+    dr[6], di[6] = 0.006, 0.007                         # |rho| < 0.01: pruned
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, scales, rot, dr, di), "cpu")
+    grad = torch.zeros(n, 3)
+    grad[0, 0] = 1.0
+    noise = torch.randn(n, 6, generator=g)
+    cfg = sense.FitConfig(max_points=10_000)
+    keeps = []
+    events = sense.density_control(p, grad, cfg, None, keeps.append, noise=noise)
+    assert events == 2 and p.n == n + 1 - 1
+    # after the split: rows 1..n-1, then the two children; then row 6 pruned
+    s0 = torch.exp(torch.log(torch.tensor(0.05)))
+    a = pos[0] + noise[0, :3] * s0 * 0.5
+    b = pos[0] + noise[0, 3:] * s0 * 0.5
+    assert torch.equal(p.positions[-2], a) and torch.equal(p.positions[-1], b)
+    assert torch.allclose(torch.exp(p.log_scales[-1]), torch.full((3,), 0.05 / 1.6), rtol=1e-6)
+    assert not torch.isclose(p.density_r, torch.tensor(0.006)).logical_and(
+        torch.isclose(p.density_i, torch.tensor(0.007))).any()
+    assert torch.isclose(p.density_i, torch.tensor(0.008)).sum() == 1
