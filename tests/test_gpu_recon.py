@@ -13,7 +13,7 @@ import os
 import pytest
 import torch
 
-from gs_tmi_b200 import sense, synthetic
+from gs_tmi_b200 import density, sense, synthetic
 from tests.helpers_ref import REF, RefVoxelizer
 
 pytestmark = pytest.mark.gpu
@@ -85,6 +85,11 @@ def test_full_plain_reconstruction_128x128x96(cuda_device):
     r3 = sense.fit(case, init, dataclasses.replace(cfg, fused_sense=False), device=str(cuda_device), eval_ssim=False)
     report["this_build_torch_data_term"] = {"seconds": r3.seconds, "final_nmse": r3.final_nmse,
                                             "n_points": r3.params.n}
+    for name, fn in (("this_build_graph", sense.fit_graph), ("this_build_live_rows", density.fit_live)):
+        st = {}
+        r = fn(case, init, dataclasses.replace(cfg, capturable_adam=True), device=str(cuda_device), eval_ssim=False,
+               stats=st)
+        report[name] = {"seconds": r.seconds, "final_nmse": r.final_nmse, "n_points": r.params.n, "stats": st}
     report["reference_rerun_nmse_rel_diff"] = r2.final_nmse / report["reference_kernels"]["final_nmse"] - 1
     report["wall_speedup"] = report["reference_kernels"]["seconds"] / report["this_build"]["seconds"]
     report["nmse_rel_diff"] = report["this_build"]["final_nmse"] / report["reference_kernels"]["final_nmse"] - 1

@@ -48,10 +48,13 @@ def rel(a, b):
     return float((a.double().cpu() - b).norm() / b.norm().clamp_min(1e-30))
 
 
-def test_mlp_forward_backward_vs_cpu(cuda_device):
+@pytest.mark.parametrize("B", [1536, 28125, 50000])
+def test_mlp_forward_backward_vs_cpu(B, cuda_device):
+    """B = 1536: every split-K slice fits the 4-stage ring; 28,125 (a 96^3
+    training phantom's seed count, 7 k-tiles per slice) and 50,000 (13 per
+    slice): the ring refills its stages, with partial row and K tiles."""
     mlp = warmstart.WarmStartMLP(str(cuda_device), seed=1)
     g = torch.Generator(device=cuda_device).manual_seed(2)
-    B = 1536
     x = torch.randn(B, 256, device=cuda_device, generator=g).bfloat16()
     dout = torch.randn(B, 16, device=cuda_device, generator=g) / B
     out, cache = mlp.forward(x)
