@@ -113,6 +113,8 @@ SIGNATURES = {
     "gsv_density_control": (ctypes.c_int, [ctypes.POINTER(GsvDensityRows), _vp, _vp,
                                            ctypes.POINTER(GsvDensityConfig), _vp, _vp, _vp, _sz, _vp]),
     "gsv_normal_fill": (ctypes.c_int, [_vp, _i64, ctypes.c_uint64, _vp, _vp]),
+    "gsv_poisson_workspace_bytes": (_sz, [_i32, _i32, _i32]),
+    "gsv_poisson_masks": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i64, _i32, _vp, _vp, _vp, _sz, _vp]),
     "gsv_knn3_mean_distance": (ctypes.c_int, [_vp, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_forward": (ctypes.c_int, [_vp] * 7 + [_i64, _i64, _i32, _i32, _i32, _i32, _vp, _vp, _vp]),
     "gsv_tile_backward": (ctypes.c_int, [_vp] * 9 + [_i64, _i64, _i32, _i32, _i32, _i32] + [_vp] * 5),

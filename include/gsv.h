@@ -349,6 +349,23 @@ GSV_API int gsv_density_control(const gsv_density_rows* rows, const float* pos_g
  * (torch.randn_like at gaussian_model.py:135-136). */
 GSV_API int gsv_normal_fill(float* out, int64_t count, uint64_t seed, int64_t* counter, void* stream);
 
+/* V/data/mask_generator.py:241-390 (_generate_poisson_mask_heuristic), for
+ * `count` masks in one launch: variable-density Poisson-disc (ky, kz) masks
+ * of ny x nz pixels (ny*nz <= 196608).  radius [ny*nz] FP64: the exclusion
+ * radius per pixel (the reference's r_grid = 0.6 / sqrt(max(pdf, 1e-4)));
+ * orders [count, ny*nz] int32: each mask's pixel visiting order (the
+ * reference's np.random.permutation); calib: the calibration square's edge
+ * (Python slice semantics around ny/2, nz/2); target: pixels to set
+ * (int(ny*nz/accel)).  masks [count, ny*nz] int8 out; rounds [count] int32
+ * out (may be NULL): parallel rounds used, -1 if that order is not a
+ * permutation (its mask is then the calibration square).  Equal to the
+ * reference's sequential pass for the same order.  ws: device scratch of
+ * gsv_poisson_workspace_bytes(ny, nz, count) bytes (0: unsupported size). */
+GSV_API size_t gsv_poisson_workspace_bytes(int32_t ny, int32_t nz, int32_t count);
+GSV_API int gsv_poisson_masks(const double* radius, const int32_t* orders, int32_t ny, int32_t nz, int32_t calib,
+                              int64_t target, int32_t count, int8_t* masks, int32_t* rounds, void* ws,
+                              size_t ws_bytes, void* stream);
+
 /* V/gaussian/gaussian_model.py:283-306 (_sampled_3nn_scale_init, a cKDTree on
  * the CPU): for n distinct seed voxels (flat row-major indices into the
  * (d,h,w) volume) with their FP32 normalised positions [n,3]

@@ -710,3 +710,69 @@ ORC_EXPORT int64_t orc_extent_check(const float* pos, const float* scl, const fl
     }
     return bad;
 }
+
+/* ------------------------------------------------------------------ */
+/* Variable-density Poisson-disc k-space mask                           */
+/* ------------------------------------------------------------------ */
+
+/* Python slice bounds [start, stop) of `start:stop` on an axis of size n
+ * (negative indices count from the end; both clipped to [0, n]). */
+static void py_slice(int64_t start, int64_t stop, int64_t n, int64_t* lo, int64_t* hi) {
+    if (start < 0) start += n;
+    if (stop < 0) stop += n;
+    if (start < 0) start = 0;
+    if (stop < 0) stop = 0;
+    if (start > n) start = n;
+    if (stop > n) stop = n;
+    *lo = start;
+    *hi = stop > start ? stop : start;
+}
+
+/* V/data/mask_generator.py:241-390 (_generate_poisson_mask_heuristic):
+ * the calibration square set first, then one pass of dart throwing over the
+ * pixels in `order` (the reference's np.random.permutation): a pixel is
+ * taken unless it is already set or an already taken pixel lies at squared
+ * distance < radius^2 (radius = the reference's r_grid = 0.6 / sqrt(pdf)),
+ * until `target` pixels are set.  Sequential, as the reference; returns the
+ * number of pixels set. */
+ORC_EXPORT int64_t orc_poisson_mask(const double* radius, const int32_t* order, int32_t ny, int32_t nz,
+                                    int32_t calib, int64_t target, int8_t* mask) {
+    const int64_t n = (int64_t)ny * nz;
+    memset(mask, 0, (size_t)n);
+    const int64_t cy = ny / 2, cz = nz / 2, h = calib / 2;
+    int64_t y0, y1, z0, z1;
+    py_slice(cy - h, cy + h, ny, &y0, &y1);
+    py_slice(cz - h, cz + h, nz, &z0, &z1);
+    int64_t count = 0;
+    for (int64_t y = y0; y < y1; ++y)
+        for (int64_t z = z0; z < z1; ++z) {
+            mask[y * nz + z] = 1;
+            ++count;
+        }
+    if (count >= target) return count;
+    for (int64_t i = 0; i < n; ++i) {
+        if (count >= target) break;
+        const int64_t c = order[i];
+        const int64_t y = c / nz, z = c % nz;
+        if (mask[c]) continue;
+        const double r = radius[c];
+        const int64_t ir = (int64_t)ceil(r);
+        const int64_t ya = y - ir > 0 ? y - ir : 0, yb = y + ir + 1 < ny ? y + ir + 1 : ny;
+        const int64_t za = z - ir > 0 ? z - ir : 0, zb = z + ir + 1 < nz ? z + ir + 1 : nz;
+        const double r2 = r * r;
+        int clash = 0;
+        for (int64_t py = ya; py < yb && !clash; ++py)
+            for (int64_t pz = za; pz < zb; ++pz) {
+                if (!mask[py * nz + pz]) continue;
+                const double d2 = (double)((py - y) * (py - y) + (pz - z) * (pz - z));
+                if (d2 < r2) {
+                    clash = 1;
+                    break;
+                }
+            }
+        if (clash) continue;
+        mask[c] = 1;
+        ++count;
+    }
+    return count;
+}

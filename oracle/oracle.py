@@ -78,6 +78,9 @@ def lib():
             L.orc_extent_check.argtypes = [_f32p, _f32p, _f32p, _i64, _i32, _i32, _i32, _i32p, _i32p,
                                            np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")]
             L.orc_extent_check.restype = _i64
+            L.orc_poisson_mask.argtypes = [_f64p, _i32p, _i32, _i32, _i32, _i64,
+                                           np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")]
+            L.orc_poisson_mask.restype = _i64
             L.orc_num_threads.argtypes = []
             L.orc_num_threads.restype = ctypes.c_int
             _lib = L
@@ -265,3 +268,15 @@ def extent_check(positions, scales, rotations, shape, tile_ranges, pair_ids):
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+def poisson_mask(radius, order, shape, calib, target):
+    """Sequential variable-density Poisson-disc dart throwing
+    (3DGS/3dgsVC/data/mask_generator.py:241-390): int8 [ny, nz] mask for the
+    exclusion radius map `radius` (FP64 [ny, nz]) and pixel visiting order
+    `order` (a permutation of ny*nz)."""
+    ny, nz = shape
+    out = np.zeros(ny * nz, np.int8)
+    lib().orc_poisson_mask(_c(radius, np.float64).reshape(-1), _c(order, np.int32), ny, nz, int(calib),
+                           int(target), out)
+    return out.reshape(ny, nz)
