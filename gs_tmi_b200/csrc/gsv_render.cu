@@ -516,13 +516,14 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
             const float e2[8] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, eb.z, eb.w};
             const float e1 = __fsub_rn(ev1, g.c1);
             const float hr = -0.5f * g.rho_r, hi = -0.5f * g.rho_i;
-            float e0[RPL], R0[RPL], R1[RPL], R2[RPL];
-            float Dr = 0.f, Di = 0.f;
+            // per row: Dr/Di = sum w g_r / g_i; R1/R2 = sum a e2 / a e2^2 with
+            // a = w (hr g_r + hi g_i); sum a itself = hr Dr + hi Di (after the loop)
+            float e0[RPL], Dr[RPL], Di[RPL], R1[RPL], R2[RPL];
             bool wany = false;
 #pragma unroll
             for (int r = 0; r < RPL; ++r) {
                 e0[r] = __fsub_rn(ev0[r], g.c0);
-                R0[r] = R1[r] = R2[r] = 0.f;
+                Dr[r] = Di[r] = R1[r] = R2[r] = 0.f;
                 if (!(bits & (1 << r))) continue;  // slot out of the Gaussian's extent
                 const float A = row_a(g, e0[r], e1), B = row_b(g, e0[r], e1);
                 float m[8];
@@ -539,11 +540,9 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                     const int q = r * 8 + k;
                     if (m[k] <= kCut) {
                         const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
-                        const float av = wgt * fmaf(hi, gi[q], hr * gr[q]);
-                        Dr = fmaf(wgt, gr[q], Dr);
-                        Di = fmaf(wgt, gi[q], Di);
-                        R0[r] += av;
-                        const float ae = av * e2[k];
+                        Dr[r] = fmaf(wgt, gr[q], Dr[r]);
+                        Di[r] = fmaf(wgt, gi[q], Di[r]);
+                        const float ae = wgt * fmaf(hi, gi[q], hr * gr[q]) * e2[k];
                         R1[r] += ae;
                         R2[r] = fmaf(ae, e2[k], R2[r]);
                     }
@@ -557,9 +556,13 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                 continue;
             }
             float v[16];
-            float R0s = 0.f, R1s = 0.f, R2s = 0.f, S1 = 0.f, S2 = 0.f, S3 = 0.f;
+            float Drs = 0.f, Dis = 0.f, R0s = 0.f, R1s = 0.f, R2s = 0.f, S1 = 0.f, S2 = 0.f, S3 = 0.f;
+            float R0[RPL];
 #pragma unroll
             for (int r = 0; r < RPL; ++r) {
+                R0[r] = fmaf(hi, Di[r], hr * Dr[r]);
+                Drs += Dr[r];
+                Dis += Di[r];
                 R0s += R0[r];
                 R1s += R1[r];
                 R2s += R2[r];
@@ -567,8 +570,8 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                 S2 = fmaf(e0[r] * e0[r], R0[r], S2);  // sum a e0^2
                 S3 = fmaf(e0[r], R1[r], S3);          // sum a e0 e2
             }
-            v[0] = Dr;
-            v[1] = Di;
+            v[0] = Drs;
+            v[1] = Dis;
             v[2] = S1;
             v[3] = e1 * R0s;
             v[4] = R1s;
