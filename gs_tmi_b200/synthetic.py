@@ -221,11 +221,14 @@ class MRICase:
 
 
 def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise_rel: float = 1e-3,
-             seed: int = 0, device=None) -> MRICase:
+             seed: int = 0, device=None, mask_kind: str = "vd") -> MRICase:
     """Synthetic multi-coil acquisition: phantom x coils -> fft3c -> mask +
     complex noise sigma = noise_rel * max|k| -> SENSE-combined zero-filled.
     `device`: where the FFTs and the noise are computed (and the case lives);
-    the default, the CPU, is the reference generator of all seeded cases."""
+    the default, the CPU, is the reference generator of all seeded cases.
+    `mask_kind`: "vd" (variable_density_mask, any device) or "poisson" (the
+    reference's own Poisson-disc generator, mask_generator.py:241-400, on
+    the GPU through gs_tmi_b200.masks; visiting order drawn with seed + 3)."""
     dev = torch.device(device) if device is not None else torch.device("cpu")
     x = ellipsoid_phantom(shape, seed=seed).to(dev)
     S = ring_coils(shape, n_coils, seed=seed + 1).to(dev)
@@ -234,7 +237,16 @@ def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise
     sigma = noise_rel * float(k.abs().max())
     noise = torch.complex(torch.randn(k.shape, generator=g, device=dev),
                           torch.randn(k.shape, generator=g, device=dev)) * sigma
-    m = variable_density_mask(shape, accel, calib, seed=seed + 3).to(dev)
+    if mask_kind == "poisson":
+        from . import masks
+
+        plane = masks.poisson_masks(tuple(shape[1:]), accel, calib, seeds=[seed + 3],
+                                    device=dev if dev.type == "cuda" else "cuda")[0]
+        m = masks.expand_phase_mask(plane.float().to(dev), tuple(shape), (1, 2))
+    elif mask_kind == "vd":
+        m = variable_density_mask(shape, accel, calib, seed=seed + 3).to(dev)
+    else:
+        raise ValueError(f"unknown mask kind {mask_kind!r}")
     ku = (k + noise) * m.unsqueeze(0)
     zf = (torch.conj(S) * ifft3c(ku)).sum(0)
     return MRICase(x, S, m, ku.to(torch.complex64), zf.to(torch.complex64))

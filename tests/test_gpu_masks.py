@@ -76,3 +76,18 @@ def test_edge_cases(cuda_device):
     m2 = torch.tensor([[1, 0], [0, 1]], dtype=torch.float32)
     e = masks.expand_phase_mask(m2, (3, 2, 2), (1, 2))
     assert e.shape == (3, 2, 2) and torch.equal(e[1], m2)
+
+
+def test_mri_case_with_the_reference_mask(cuda_device):
+    """synthetic.mri_case(mask_kind="poisson"): the (ky, kz) plane is the
+    reference generator's mask for the order RandomState(seed + 3) draws,
+    repeated along the fully sampled readout axis."""
+    from gs_tmi_b200 import synthetic
+
+    shape, accel, calib, seed = (12, 48, 40), 6.0, 12, 5
+    case = synthetic.mri_case(shape, n_coils=2, accel=accel, calib=calib, seed=seed, mask_kind="poisson")
+    order = np.random.RandomState(seed + 3).permutation(48 * 40).astype(np.int32)
+    ref = oracle.poisson_mask(masks.exclusion_radius((48, 40), accel, calib), order, (48, 40), calib,
+                              masks.target_points((48, 40), accel))
+    m = case.mask.numpy()
+    assert m.shape == shape and all(np.array_equal(m[i], ref) for i in range(shape[0]))

@@ -71,7 +71,7 @@ def test_recon_parity_with_reference_kernels(cuda_device):
 @pytest.mark.skipif(os.environ.get("GSV_RECON_FULL") != "1" or REF is None, reason="set GSV_RECON_FULL=1")
 def test_full_plain_reconstruction_128x128x96(cuda_device):
     shape = (128, 128, 96)
-    case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=0)
+    case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=0, mask_kind="poisson")
     init = synthetic.from_image_init(case.zero_filled, 50_000, seed=0)
     cfg = sense.FitConfig(iterations=2000, eval_every=100, max_points=500_000)
     report = {}
@@ -90,6 +90,7 @@ def test_full_plain_reconstruction_128x128x96(cuda_device):
         r = fn(case, init, dataclasses.replace(cfg, capturable_adam=True), device=str(cuda_device), eval_ssim=False,
                stats=st)
         report[name] = {"seconds": r.seconds, "final_nmse": r.final_nmse, "n_points": r.params.n, "stats": st}
+    report["mask"] = {"kind": "poisson (reference generator)", "sampled_fraction": float(case.mask.mean())}
     report["reference_rerun_nmse_rel_diff"] = r2.final_nmse / report["reference_kernels"]["final_nmse"] - 1
     report["wall_speedup"] = report["reference_kernels"]["seconds"] / report["this_build"]["seconds"]
     report["nmse_rel_diff"] = report["this_build"]["final_nmse"] / report["reference_kernels"]["final_nmse"] - 1
