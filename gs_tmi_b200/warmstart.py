@@ -20,8 +20,8 @@ package's voxelizer and back-propagates the relative L2 distance to that
 volume through the voxelizer's backward kernels, the decoding and the MLP's
 tcgen05 backward (``render_step``).  The intensity-seeded initialisation of
 the reference (``synthetic.from_image_init``) stays as the fallback -- an
-untrained network reproduces it exactly -- and as the judge through the
-final NMSE against the fully sampled phantom.
+untrained network reproduces it exactly -- and as the yardstick: the warm
+start is scored by the final NMSE against the fully sampled phantom.
 """
 from __future__ import annotations
 
