@@ -213,6 +213,7 @@ class WarmConfig:
     accel: float = 6.0
     calib: int = 24
     points_per_voxel: float = 50_000 / (128 * 128 * 96)
+    mask_kind: str = "vd"  # "poisson": the reference's Poisson-disc (ky, kz) sampling (synthetic.mri_case)
     fit_iterations: int = 1000
 
 
@@ -242,7 +243,8 @@ def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device):
 def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
     """A synthetic phantom, its intensity-seeded Gaussians and the volume the
     plain method reconstructs from them (the training target)."""
-    case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed)
+    case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed,
+                              mask_kind=wc.mask_kind)
     n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
     x, vox, base, scale = case_inputs(case, n, seed + 1, device)
     cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=10 ** 9)

@@ -122,7 +122,8 @@ def test_warm_start_gains_over_intensity_seeding(cuda_device):
 @pytest.mark.skipif(os.environ.get("GSV_WARM_FULL") != "1", reason="set GSV_WARM_FULL=1")
 def test_full_time_to_nmse(cuda_device):
     dev = str(cuda_device)
-    wc = warmstart.WarmConfig()
+    mask_kind = os.environ.get("GSV_WARM_MASK", "vd")  # "poisson": the reference's Poisson-disc sampling
+    wc = warmstart.WarmConfig(mask_kind=mask_kind)
     n_train = int(os.environ.get("GSV_WARM_TRAIN_PHANTOMS", "48"))
     n_eval = int(os.environ.get("GSV_WARM_EVAL_PHANTOMS", "4"))
     t0 = time.perf_counter()
@@ -137,7 +138,7 @@ def test_full_time_to_nmse(cuda_device):
     cfg = sense.FitConfig(iterations=2000, eval_every=25, max_points=500_000)
     rows = []
     for e in range(n_eval):
-        case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e)
+        case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e, mask_kind=mask_kind)
         plain = sense.fit(case, synthetic.from_image_init(case.zero_filled, 50_000, seed=e), cfg, device=dev,
                           eval_ssim=True)
         target = plain.final_nmse
@@ -155,7 +156,7 @@ def test_full_time_to_nmse(cuda_device):
                      "warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": it,
                      "warm_seconds_to_target": secs, "warm_init_seconds": t_init,
                      "wall_ratio": (secs / plain.seconds) if secs else None})
-    report = {"train_phantoms": n_train, "train_examples": int(sum(c.features.shape[0] for c in cases)),
+    report = {"mask": mask_kind, "train_phantoms": n_train, "train_examples": int(sum(c.features.shape[0] for c in cases)),
               "data_seconds": t_data, "train_seconds": t_train, "final_train_loss": losses[-1],
               "eval": rows}
     ratios = [r["wall_ratio"] for r in rows if r["wall_ratio"] is not None]
