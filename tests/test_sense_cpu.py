@@ -139,3 +139,44 @@ def test_split_noise_and_prune_on_cpu():
     assert not torch.isclose(p.density_r, torch.tensor(0.006)).logical_and(
         torch.isclose(p.density_i, torch.tensor(0.007))).any()
     assert torch.isclose(p.density_i, torch.tensor(0.008)).sum() == 1
+
+
+def test_density_control_branches_on_cpu():
+    """The reference's branch order (trainer.py:300-352): nothing at
+    max_points; split when it fits, else clone; clone halves the parent's
+    density and appends a copy with log(scale + 1e-8); prune only when at
+    least 100 rows survive."""
+    n = 150
+    g = torch.Generator().manual_seed(3)
+    pos = torch.rand(n, 3, generator=g) * 2 - 1
+    rot = torch.zeros(n, 4)
+    rot[:, 0] = 1.0
+    dr = torch.full((n,), 0.5)
+    di = torch.full((n,), 0.1)
+    grad = torch.zeros(n, 3)
+    grad[:4, 0] = 1.0                      # four densify candidates
+    small = torch.full((n, 3), 0.005)      # all below the scale threshold: clone
+    cfg = sense.FitConfig(max_points=10_000)
+    events = []
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, small, rot, dr, di), "cpu")
+    assert sense.density_control(p, grad, cfg, None, events.append) == 1 and p.n == n + 4
+    assert torch.equal(p.density_r[:4], torch.full((4,), 0.25)) and torch.equal(p.density_r[n:], p.density_r[:4])
+    assert torch.equal(p.positions[n:], pos[:4])
+    assert torch.allclose(p.log_scales[n:], torch.log(torch.full((4, 3), 0.005) + 1e-8))
+    # at max_points nothing happens, not even a prune
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, small, rot, dr * 0, di * 0), "cpu")
+    assert sense.density_control(p, grad, sense.FitConfig(max_points=n), None, events.append) == 0 and p.n == n
+    # a split that would pass max_points falls back to clone; cloning off: nothing but the prune test
+    big = torch.full((n, 3), 0.05)
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, big, rot, dr, di), "cpu")
+    cfg2 = sense.FitConfig(max_points=n + 3, use_cloning=False)
+    assert sense.density_control(p, grad, cfg2, None, events.append, noise=torch.zeros(n, 6)) == 0 and p.n == n
+    # prune needs 100 survivors: 60 survivors -> no prune
+    weak = dr.clone()
+    weak[60:] = 0.001
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, big, rot, weak, di * 0), "cpu")
+    assert sense.density_control(p, torch.zeros(n, 3), cfg, None, events.append) == 0 and p.n == n
+    weak[110:] = 0.001
+    weak[60:110] = 0.5
+    p = sense.GaussianParams(synthetic.GaussianSet(pos, big, rot, weak, di * 0), "cpu")
+    assert sense.density_control(p, torch.zeros(n, 3), cfg, None, events.append) == 1 and p.n == 110
