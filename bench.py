@@ -74,9 +74,28 @@ def whole_job_rate(units_per_step, steps, world, total_ms):
     return units_per_step * steps * world / (total_ms * 1e-3)
 
 
-def make_inputs(name):
-    from gs_tmi_b200 import synthetic
+def _synthetic(standalone=False):
+    """The seeded-input generator (gs_tmi_b200/synthetic.py).  `standalone`:
+    load the file on its own, without importing the package (whose import
+    maps the product library) -- the reference arm uses no product code."""
+    if not standalone:
+        from gs_tmi_b200 import synthetic
 
+        return synthetic
+    import importlib.util
+
+    name = "gsv_seeded_inputs"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "gs_tmi_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_inputs(name, standalone=False):
+    synthetic = _synthetic(standalone)
     wl = WORKLOADS[name]
     if wl["kind"] == "from_image":
         case = synthetic.mri_case(wl["shape"], n_coils=8, accel=6.0, calib=24, seed=0)
@@ -398,7 +417,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     name = args.workload
-    gs, gv = make_inputs(name)
+    gs, gv = make_inputs(name, standalone=True)
     shape = WORKLOADS[name]["shape"]
     vals, times = [], []
     steps, warm = args.steps, args.warmup
@@ -420,187 +439,304 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+class Workload:
+    """One workload bound to the device: inputs, binning plan, tuned
+    execution shape and the three phases of a step as closures."""
+
+    def __init__(self, name, dev, args, flags):
+        from gs_tmi_b200._lib import GsvGrads, GsvParams, check, lib
+        from gs_tmi_b200.tile_voxelizer import _ptr, _shape, _stream, prepare_and_bin, work_census
+
+        self.name, self.dev = name, dev
+        self.shape = shape = WORKLOADS[name]["shape"]
+        self.gs, self.gv = make_inputs(name)
+        n = self.n = self.gs.n
+        params = self.params = tuple(t.to(dev).contiguous() for t in self.gs.tensors())
+        gvd = self.gvd = self.gv.to(dev).contiguous()
+        gshape = _shape(shape, TILE)
+        plan = self.plan = prepare_and_bin(params, gshape, flags)  # sizes the pair workspace (untimed sync)
+        cap = plan.capacity
+        self.total = plan.total
+        outs = self.outs = [torch.empty_like(t) for t in params]
+        vol = self.vol = torch.empty(shape, dtype=torch.complex64, device=dev)
+        gp = GsvParams(*(t.data_ptr() for t in params), n)
+        gg = GsvGrads(*(o.data_ptr() for o in outs))
+        st = _stream(dev)
+        wsg, wsp = _ptr(plan.ws_gauss), _ptr(plan.ws_pairs)
+        self.tuning, self.tune_times, self.tile_pick, self.tile_times = None, {}, None, {}
+        if not args.no_autotune:
+            from gs_tmi_b200.autotune import Autotuner
+
+            tuner = Autotuner()
+            self.tuning = tuner.pick(plan, params)  # untimed: times every execution shape once
+            self.tune_times = next(iter(tuner.timings.values()), {})
+            # the tile-edge comparison is reported; the workload's unit stays the reference's 8^3 tiles
+            self.tile_pick, _, self.tile_times = tuner.pick_tile_size(params, shape, flags)
+        tref = ctypes.byref(self.tuning) if self.tuning is not None else None
+
+        def prep_bin():
+            check(lib.gsv_prepare(ctypes.byref(gp), gshape, wsg, plan.gauss_bytes, None, st), "prepare")
+            check(lib.gsv_bin(gshape, n, wsg, wsp, plan.pair_bytes, cap, st), "bin")
+
+        def fwd():
+            check(lib.gsv_forward_ex(gshape, n, wsg, wsp, cap, _ptr(vol), tref, st), "forward")
+
+        def bwd():
+            check(lib.gsv_backward_ex(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags,
+                                      tref, st), "backward")
+
+        self.prep_bin, self.fwd, self.bwd = prep_bin, fwd, bwd
+        # E from the executed binning, and what the render kernels execute of it
+        tr_ptr, _ = plan.views()
+        ntiles = lib.gsv_num_tiles(gshape)
+        off = tr_ptr - plan.ws_gauss.data_ptr()
+        tr_host = plan.ws_gauss[off:off + 8 * ntiles].view(torch.int32).reshape(-1, 2).cpu().numpy()
+        self.evals = evals_of(tr_host, shape)
+        self.census = work_census(plan)
+
+    def step(self):
+        self.prep_bin()
+        self.fwd()
+        self.bwd()
+
+    def time(self, steps, warmup, flush, dist=None):
+        """Per-step device times (ms) of binning, forward and backward, CUDA
+        events on the launching stream, L2 flushed between steps."""
+        dev = self.dev
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize(dev)
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+        cur = torch.cuda.current_stream(dev)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(cur)
+            self.prep_bin()
+            ev[i][1].record(cur)
+            self.fwd()
+            ev[i][2].record(cur)
+            self.bwd()
+            ev[i][3].record(cur)
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        _, fl = self.plan.read_status(torch_stream(dev))
+        if fl:
+            raise RuntimeError(f"voxelizer status flags {fl} during the timed region")
+        return {"step": [ev[i][0].elapsed_time(ev[i][3]) for i in range(steps)],
+                "bin": [ev[i][0].elapsed_time(ev[i][1]) for i in range(steps)],
+                "fwd": [ev[i][1].elapsed_time(ev[i][2]) for i in range(steps)],
+                "bwd": [ev[i][2].elapsed_time(ev[i][3]) for i in range(steps)]}
+
+    def execution(self):
+        if self.tuning is None:
+            return "default"
+        return {"rows_per_lane": self.tuning.rows_per_lane, "chunk": self.tuning.chunk,
+                "autotune_ms_per_candidate": self.tune_times, "tile_edge_step_ms": self.tile_times,
+                "tile_edge_fastest": self.tile_pick}
+
+
+def torch_stream(dev):
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def roofline_of(wl, t, peak_ops, pk, pk_kind, sm_mhz):
+    """FP32-issue roofline of the dominant kernel (the backward) on USEFUL
+    work: the included candidates (Mahalanobis <= 9, counted on the device
+    by the work census) times the algorithmic FP32 operations each one
+    needs, over the backward's CUDA-event time.  Candidates outside the
+    cutoff do no useful work, so they count nothing here."""
+    d, h, w = wl.shape
+    bwd_ms, fwd_ms = statistics.mean(t["bwd"]), statistics.mean(t["fwd"])
+    useful = wl.census["included"]
+    ach_bwd = useful * OPS_BWD / (bwd_ms * 1e-3)
+    ach_fwd = useful * OPS_FWD / (fwd_ms * 1e-3)
+    traffic, pipes = None, None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        rec = json.load(open(tpath)).get(wl.name, {})
+        traffic, pipes = rec.get("k_backward8"), rec.get("k_backward8_pipes")
+    vol_bytes = 2 * 8 * d * h * w  # write the volume, read its gradient
+    c = wl.census
+    return {"bound": "fp32_issue", "kernel": "gsv_backward (k_backward8 + k_finalize)",
+            "achieved": ach_bwd / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s", "frac": ach_bwd / peak_ops,
+            "traffic": traffic, "ops_per_eval": OPS_BWD, "units": "included candidates (m <= 9)",
+            "units_per_launch": useful,
+            "peak_source": f"{SMS} SMs x {LANES} FP32 lanes x sm_max_mhz {sm_mhz:.0f} ({pk_kind} peaks)",
+            "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
+            "work": {"candidates": wl.evals, "included": useful, "evaluated_after_cull": c["evaluated"],
+                     "exp_block_lanes": c["exp_block_lanes"], "empty_kept_slots": c["empty_kept_slots"],
+                     "lane_efficiency": useful / max(c["exp_block_lanes"], 1)},
+            "pipes_ncu": pipes,
+            "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9, "peak_gbs": pk.get("hbm_gbs")}}
+
+
+def reference_cuda_baseline(wl, flush, reps):
+    """The reference's own CUDA voxelizer (compiled from its sources into
+    oracle/_ref/) on the same B200 and the same inputs: its forward and
+    backward kernels alone, and its full step (torch preprocess, torch
+    binning with the host sync, kernels, autograd tail), next to this
+    build's kernels and full step through the public module.  Median of
+    `reps` CUDA-event timings, L2 flushed before each."""
+    try:
+        from oracle import ref_cuda, torch_port
+    except Exception as exc:  # noqa: BLE001
+        return {"unavailable": f"reference extension not loadable: {exc}"}
+    if ref_cuda.REF is None:
+        return {"unavailable": "reference extension not built (oracle/build_ref.py needs the reference sources)"}
+    import gs_tmi_b200
+
+    REF = ref_cuda.REF
+    dev, shape = wl.dev, wl.shape
+    d, h, w = shape
+    params, g = wl.params, wl.gvd
+    with torch.no_grad():
+        center, cov_inv, half = torch_port.preprocess(*params[:3], shape)
+        tr, pid = torch_port.build_tile_pairs_torch(center, torch_port.radius_vox(params[1], half), shape, TILE)
+    gr, gi = g.real.contiguous(), g.imag.contiguous()
+    dr, di = params[3], params[4]
+
+    def ref_kernels():
+        REF.forward(center, cov_inv, dr, di, tr, pid, half, TILE, d, h, w)
+        REF.backward(center, cov_inv, dr, di, tr, pid, half, gr, gi, TILE, d, h, w)
+
+    def ref_full():
+        ps = [p.detach().requires_grad_(True) for p in params]
+        ref_cuda.reference_step(ps, shape, TILE).backward(g)
+
+    def our_full():
+        ps = [p.detach().requires_grad_(True) for p in params]
+        gs_tmi_b200.voxelize(*ps, shape, TILE).backward(g)
+
+    def timed(fn):
+        fn()
+        out = []
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            out.append(e0.elapsed_time(e1))
+        return statistics.median(out)
+
+    r = {"ref_kernels_ms": timed(ref_kernels), "kernels_ms": timed(lambda: (wl.fwd(), wl.bwd())),
+         "ref_full_step_ms": timed(ref_full), "full_step_ms": timed(our_full)}
+    r["speedup_kernels"] = r["ref_kernels_ms"] / r["kernels_ms"]
+    r["speedup_full_step"] = r["ref_full_step_ms"] / r["full_step_ms"]
+    r["reps"] = reps
+    r["what"] = ("kernels: forward + backward launches alone (this build: autotuned shape, atomic backward + "
+                 "finalize to raw-parameter gradients; reference: its two kernels, gradients to center/cov_inv); "
+                 "full step: preprocess + binning + forward + backward through each build's public module, "
+                 "autograd included")
+    return r
+
+
 def run_ours(args, rank, world, dist):
     from gs_tmi_b200 import TileVoxelizer
-    from gs_tmi_b200._lib import GSV_BACKWARD_DETERMINISTIC, GsvGrads, GsvParams, check, lib
-    from gs_tmi_b200.tile_voxelizer import _ptr, _shape, _stream, prepare_and_bin
+    from gs_tmi_b200._lib import GSV_BACKWARD_DETERMINISTIC
 
     local = int(os.environ.get("LOCAL_RANK", 0))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     name = args.workload
-    shape = WORKLOADS[name]["shape"]
-    gs, gv = make_inputs(name)
-    n = gs.n
     flags = GSV_BACKWARD_DETERMINISTIC if args.deterministic else 0
-    params = tuple(t.to(dev).contiguous() for t in gs.tensors())
-    gvd = gv.to(dev).contiguous()
-    gshape = _shape(shape, TILE)
-    plan = prepare_and_bin(params, gshape, flags)  # sizes the pair workspace (one sync, untimed)
-    cap, total = plan.capacity, plan.total
-    tr_host = None
-    outs = [torch.empty_like(t) for t in params]
-    vol = torch.empty(shape, dtype=torch.complex64, device=dev)
-    gp = GsvParams(*(t.data_ptr() for t in params), n)
-    gg = GsvGrads(*(o.data_ptr() for o in outs))
-    st = _stream(dev)
-    wsg, wsp = _ptr(plan.ws_gauss), _ptr(plan.ws_pairs)
-
-    def prep_bin():
-        check(lib.gsv_prepare(ctypes.byref(gp), gshape, wsg, plan.gauss_bytes, None, st), "prepare")
-        check(lib.gsv_bin(gshape, n, wsg, wsp, plan.pair_bytes, cap, st), "bin")
-
-    tuning = None
-    if not args.no_autotune:
-        from gs_tmi_b200.autotune import Autotuner
-
-        tuner = Autotuner()
-        tuning = tuner.pick(plan, params)  # untimed: times every execution shape once
-        tune_times = next(iter(tuner.timings.values()), {})
-        # the tile-edge comparison is reported; the workload's unit stays the reference's 8^3 tiles
-        tile_pick, _, tile_times = tuner.pick_tile_size(params, shape, flags)
-    tref = ctypes.byref(tuning) if tuning is not None else None
-
-    def fwd():
-        check(lib.gsv_forward_ex(gshape, n, wsg, wsp, cap, _ptr(vol), tref, st), "forward")
-
-    def bwd():
-        check(lib.gsv_backward_ex(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags, tref,
-                                  st), "backward")
-
-    def step():
-        prep_bin()
-        fwd()
-        bwd()
-
-    # E from the executed binning
-    tr_ptr, _ = plan.views()
-    ntiles = lib.gsv_num_tiles(gshape)
-    off = tr_ptr - plan.ws_gauss.data_ptr()
-    tr_host = plan.ws_gauss[off:off + 8 * ntiles].view(torch.int32).reshape(-1, 2).cpu().numpy()
-    d, h, w = shape
-    nvox = []
-    for t in range(ntiles):
-        td, rem = divmod(t, (-(-h // TILE)) * (-(-w // TILE)))
-        th, tw = divmod(rem, -(-w // TILE))
-        nvox.append(min(TILE, d - td * TILE) * min(TILE, h - th * TILE) * min(TILE, w - tw * TILE))
-    evals = int(((tr_host[:, 1] - tr_host[:, 0]).astype(np.int64) * np.array(nvox)).sum())
-
+    wl = Workload(name, dev, args, flags)
+    shape, gs, gv, n = wl.shape, wl.gs, wl.gv, wl.n
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     for _ in range(args.warmup):
-        step()
+        wl.step()
     torch.cuda.synchronize(dev)
-    n_launch, kernel_names = (None, []) if args.no_launch_count else count_library_launches(step, dev)
+    n_launch, kernel_names = (None, []) if args.no_launch_count else count_library_launches(wl.step, dev)
 
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    cur = torch.cuda.current_stream(dev)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.zero_()
-            ev[i][0].record(cur)
-            prep_bin()
-            ev[i][1].record(cur)
-            fwd()
-            ev[i][2].record(cur)
-            bwd()
-            ev[i][3].record(cur)
+        t = wl.time(args.steps, args.warmup, flush, dist)
+        total_ms = sum(t["step"])
+
+        # e2e through the public module with pinned host buffers
+        vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic,
+                            autotune=not args.no_autotune)
+        host_in = [x.pin_memory() for x in gs.tensors()]
+        gv_host = gv.pin_memory()
+        host_out = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in gs.tensors()]
+        vol_host = torch.empty(shape, dtype=torch.complex64).pin_memory()
+        h2d = sum(x.numel() * x.element_size() for x in host_in) + gv_host.numel() * 8
+        d2h = sum(x.numel() * x.element_size() for x in host_out) + vol_host.numel() * 8
+        up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+        def e2e_step():
+            # copies overlap compute the way a caller with two copy streams would run it:
+            # the upstream gradient uploads during binning + forward, the volume downloads
+            # during the backward
+            main = torch.cuda.current_stream(dev)
+            ps = [x.to(dev, non_blocking=True).requires_grad_(True) for x in host_in]
+            up.wait_stream(main)
+            with torch.cuda.stream(up):
+                g = gv_host.to(dev, non_blocking=True)
+            v = vox(ps[0], ps[1], ps[2], torch.complex(ps[3], ps[4]))
+            down.wait_stream(main)
+            with torch.cuda.stream(down):
+                vol_host.copy_(v.detach(), non_blocking=True)
+            main.wait_stream(up)
+            g.record_stream(main)
+            v.backward(g)
+            for o, p in zip(host_out, ps):
+                o.copy_(p.grad, non_blocking=True)
+            main.wait_stream(down)
+
+        for _ in range(args.warmup):
+            e2e_step()
         torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    t_step = [ev[i][0].elapsed_time(ev[i][3]) for i in range(args.steps)]
-    t_bin = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
-    t_fwd = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
-    t_bwd = [ev[i][2].elapsed_time(ev[i][3]) for i in range(args.steps)]
-    total_ms = sum(t_step)
-    _, fl = plan.read_status(st)
-    if fl:
-        raise RuntimeError(f"voxelizer status flags {fl} during the timed region")
+        cur = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        e0.record(cur)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(cur)
+        torch.cuda.synchronize(dev)
+        e2e_ms = e0.elapsed_time(e1)
 
-    # e2e through the public module with pinned host buffers
-    vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic,
-                        autotune=not args.no_autotune)
-    host_in = [t.pin_memory() for t in gs.tensors()]
-    gv_host = gv.pin_memory()
-    host_out = [torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in gs.tensors()]
-    vol_host = torch.empty(shape, dtype=torch.complex64).pin_memory()
-    h2d = sum(t.numel() * t.element_size() for t in host_in) + gv_host.numel() * 8
-    d2h = sum(t.numel() * t.element_size() for t in host_out) + vol_host.numel() * 8
-
-    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
-
-    def e2e_step():
-        # copies overlap compute the way a caller with two copy streams would run it:
-        # the upstream gradient uploads during binning + forward, the volume downloads
-        # during the backward
-        main = torch.cuda.current_stream(dev)
-        ps = [t.to(dev, non_blocking=True).requires_grad_(True) for t in host_in]
-        up.wait_stream(main)
-        with torch.cuda.stream(up):
-            g = gv_host.to(dev, non_blocking=True)
-        v = vox(ps[0], ps[1], ps[2], torch.complex(ps[3], ps[4]))
-        down.wait_stream(main)
-        with torch.cuda.stream(down):
-            vol_host.copy_(v.detach(), non_blocking=True)
-        main.wait_stream(up)
-        g.record_stream(main)
-        v.backward(g)
-        for o, p in zip(host_out, ps):
-            o.copy_(p.grad, non_blocking=True)
-        main.wait_stream(down)
-
-    for _ in range(args.warmup):
-        e2e_step()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    e0.record(cur)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(cur)
-    torch.cuda.synchronize(dev)
-    e2e_ms = e0.elapsed_time(e1)
-
-    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
+        total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
+        extra = {}
+        if rank == 0 and world == 1 and not args.no_extras:
+            # the BASELINE voxelizer micro-benchmark (64^3, N = 20,000) on the same box
+            if name != "cube64_n20k":
+                small = Workload("cube64_n20k", dev, args, flags)
+                ts_ = small.time(args.steps, args.warmup, flush)
+                extra["cube64_n20k"] = {
+                    "value": small.evals * args.steps / (sum(ts_["step"]) * 1e-3) / 1e9, "unit": "Gvox-evals/s",
+                    "ms_per_step": sum(ts_["step"]) / args.steps, "evals_per_step": small.evals,
+                    "breakdown_ms": {"prepare_bin": statistics.mean(ts_["bin"]),
+                                     "forward": statistics.mean(ts_["fwd"]),
+                                     "backward": statistics.mean(ts_["bwd"])},
+                    "execution": small.execution(), "included": small.census["included"]}
+                del small
+            extra["reference_cuda"] = reference_cuda_baseline(wl, flush, reps=max(args.steps, 5))
     if rank != 0:
         return
     pk, pk_kind = peaks()
     clocks = clk.summary()
     sm_mhz = float(pk.get("sm_max_mhz", 1965.0))
     peak_ops = SMS * LANES * sm_mhz * 1e6
-    bwd_ms = statistics.mean(t_bwd)
-    fwd_ms = statistics.mean(t_fwd)
-    ach_bwd = evals * OPS_BWD / (bwd_ms * 1e-3)
-    ach_fwd = evals * OPS_FWD / (fwd_ms * 1e-3)
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(name, {}).get("k_backward8")
-    vol_bytes = 2 * 8 * d * h * w  # write the volume, read its gradient
+    evals = wl.evals
     value = whole_job_rate(evals, args.steps, world, total_ms) / 1e9
     out = {
         "metric": "fwd+bwd Gvox-evals/s", "value": value, "unit": "Gvox-evals/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": name, "volume": list(shape), "gaussians": n, "tile_size": TILE, "pairs": total,
+        "config": {"workload": name, "volume": list(shape), "gaussians": n, "tile_size": TILE, "pairs": wl.total,
                    "evals_per_step": evals, "deterministic": bool(args.deterministic),
-                   "execution": ({"rows_per_lane": tuning.rows_per_lane, "chunk": tuning.chunk,
-                                  "autotune_ms_per_candidate": tune_times,
-                                  "tile_edge_step_ms": tile_times, "tile_edge_fastest": tile_pick}
-                                 if tuning is not None else "default"),
+                   "execution": wl.execution(),
                    "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
-        "breakdown_ms": {"prepare_bin": statistics.mean(t_bin), "forward": fwd_ms, "backward": bwd_ms},
-        "roofline": {"bound": "fp32_issue", "kernel": "gsv_backward (k_backward8 + k_finalize)",
-                     "achieved": ach_bwd / 1e12, "peak": peak_ops / 1e12, "unit": "TOP/s",
-                     "frac": ach_bwd / peak_ops, "traffic": traffic,
-                     "ops_per_eval": OPS_BWD,
-                     "peak_source": f"{SMS} SMs x {LANES} FP32 lanes x sm_max_mhz {sm_mhz:.0f} ({pk_kind} peaks)",
-                     "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
-                     "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9,
-                             "peak_gbs": pk.get("hbm_gbs")}},
+        "breakdown_ms": {"prepare_bin": statistics.mean(t["bin"]), "forward": statistics.mean(t["fwd"]),
+                         "backward": statistics.mean(t["bwd"])},
+        "roofline": roofline_of(wl, t, peak_ops, pk, pk_kind, sm_mhz),
         "e2e": {"value": whole_job_rate(evals, args.steps, world, e2e_ms) / 1e9, "unit": "Gvox-evals/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
                 "api": "gs_tmi_b200.TileVoxelizer forward + autograd backward; upstream-gradient upload and "
@@ -609,6 +745,7 @@ def run_ours(args, rank, world, dist):
         "launches_per_step": n_launch, "kernels": kernel_names,
         "clocks": clocks,
     }
+    out.update({k: v for k, v in extra.items()})
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(gs, gv, shape)
     print(json.dumps(out), flush=True)
@@ -625,6 +762,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the CUDA activity trace (under ncu)")
     ap.add_argument("--no-autotune", action="store_true", help="default execution shape, no tuning pass")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the 64^3 line and the reference-CUDA baseline (under ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

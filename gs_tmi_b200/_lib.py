@@ -98,6 +98,7 @@ SIGNATURES = {
     "gsv_batch_setup": (ctypes.c_int, [ctypes.POINTER(GsvBatchItem), ctypes.c_int, ctypes.c_int, _vp, _sz, _vp]),
     "gsv_forward_batched": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "gsv_backward_batched": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "gsv_count_work": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, ctypes.c_void_p, _vp, _vp]),
     "gsv_build_tile_pairs_count": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _sz, _i64p, _vp]),
     "gsv_build_tile_pairs_fill": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp, _vp, _vp]),
     "gsv_build_tile_pairs_noalloc": (ctypes.c_int, [_vp, _vp, _i64, _S, _vp, _vp, _i64, _i64p, _vp]),

@@ -16,11 +16,12 @@
 //
 // In host code the array's name is only a host-side stand-in, never a device
 // address.  The first call on each device (with that device current) looks
-// up the real address with cudaGetSymbolAddress and caches it; make that
-// first call before any stream capture.  All calls share the one array and
-// it keeps the previous call's contents: the entry point clears what must
-// start at zero, and calls that overlap on the GPU (two streams or threads at
-// once) race on it, so callers must serialise them.
+// up the real address with cudaGetSymbolAddress and caches it.  The call
+// synchronises its stream once (to read the pair total back).  All calls
+// share the one array and it keeps the previous call's contents: the entry
+// point clears what must start at zero, and calls that overlap on the GPU
+// (two streams or threads at once) race on it, so callers must serialise
+// them.
 #include <cub/cub.cuh>
 
 #include <mutex>
@@ -100,27 +101,45 @@ __global__ void __launch_bounds__(256) k_na_count(const float* __restrict__ cent
 }
 
 // Pairs in Gaussian-major (d,h,w) raster order (tile_voxelizer.py:126-145).
+// A warp owns 32 consecutive Gaussians and writes their pairs as one
+// contiguous range: lane l takes pairs base + l, base + 32 + l, ... and finds
+// its Gaussian by a shuffle binary search over the warp's first indices, so
+// one large Gaussian is spread over the warp and the stores are coalesced.
 __global__ void __launch_bounds__(128) k_na_emit(const int4* __restrict__ boxes,
                                                  const int64_t* __restrict__ offsets, int64_t n, NaShape s,
                                                  int32_t* __restrict__ keys, int32_t* __restrict__ vals) {
+    constexpr unsigned kAll = 0xffffffffu;
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= n) return;
-    const int4 b = boxes[g];
-    if (b.w <= 0) return;
-    const int32_t t0 = b.x & 0xffff, t1 = (b.x >> 16) & 0xffff, t2 = b.y & 0xffff;
-    const int32_t n1 = b.z & 0xffff, n2 = (b.z >> 16) & 0xffff;
-    int64_t o = offsets[g];
-    for (int32_t i = 0, j = 0, k = 0, c = 0; c < b.w; ++c) {
-        keys[o] = ((t0 + i) * s.nt[1] + (t1 + j)) * s.nt[2] + (t2 + k);
-        vals[o] = int32_t(g);
-        ++o;
-        if (++k == n2) {
-            k = 0;
-            if (++j == n1) {
-                j = 0;
-                ++i;
-            }
+    const int lane = threadIdx.x & 31;
+    const int64_t g0 = g - lane;  // first Gaussian of this warp (warp-uniform)
+    if (g0 >= n) return;
+    const int m = int(min(int64_t(32), n - g0));
+    const long long end = offsets[g0 + m];  // one past the warp's last pair
+    int4 b = make_int4(0, 0, 0, 0);
+    long long o = end;  // lanes past the last Gaussian never match
+    if (lane < m) {
+        b = boxes[g];
+        o = offsets[g];
+    }
+    const long long start = __shfl_sync(kAll, o, 0);
+    for (long long base = start; base < end; base += 32) {
+        const long long p = base + lane;
+        int j = 0;  // largest j with o_j <= p
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+            const long long oj = __shfl_sync(kAll, o, j + step);
+            if (oj <= p) j += step;
         }
+        const long long oj = __shfl_sync(kAll, o, j);
+        const int bx = __shfl_sync(kAll, b.x, j), by = __shfl_sync(kAll, b.y, j), bz = __shfl_sync(kAll, b.z, j);
+        if (p >= end) continue;
+        const int32_t c = int32_t(p - oj);
+        const int32_t t0 = bx & 0xffff, t1 = (bx >> 16) & 0xffff, t2 = by & 0xffff;
+        const int32_t n1 = bz & 0xffff, n2 = (bz >> 16) & 0xffff;
+        const int32_t k = c % n2, r = c / n2;
+        const int32_t jj = r % n1, i = r / n1;
+        keys[p] = ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
+        vals[p] = int32_t(g0 + j);
     }
 }
 

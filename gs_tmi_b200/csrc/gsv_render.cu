@@ -1167,6 +1167,77 @@ __global__ void __launch_bounds__(256) k_gather_det_batched(const BatchTable t) 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Work census of the tile-8 kernels (diagnostic, no gradients): per listed
+// (tile, Gaussian) pair it replays the render kernels' decisions with their
+// arithmetic -- the extent cull per 4x8x8 row slot, the row-form quadratic
+// and the FP32 cutoff -- and counts
+//   out[0]  included candidates (m <= 9, voxel inside the volume),
+//   out[1]  candidates the kernels evaluate m for (voxels of kept slots),
+//   out[2]  lanes issued by the per-column exp / FMA blocks (32 per column
+//           of a kept slot in which some lane is inside the cutoff),
+//   out[3]  kept slots without any included voxel.
+// out[0] / out[2] is the lane efficiency of the exp / FMA blocks.  The
+// inclusion count covers every listed slot, culled or not, so it also checks
+// that the cull drops no included voxel.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_count_work(const RenderArgs a, unsigned long long* out) {
+    const int64_t tile = blockIdx.x;
+    const int2 rg = a.ranges[tile];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int d0, h0, w0;
+    decode_tile(a, tile, d0, h0, w0);
+    unsigned long long c_inc = 0, c_eval = 0, c_lanes = 0, c_empty = 0;
+    const float ev1 = float(h0 + (lane & 7));
+    const bool h_ok = h0 + (lane & 7) < a.h;
+    for (int p = rg.x + warp; p < rg.y; p += kWarps) {
+        const int gid = __ldg(a.pair_ids + p);
+        float ih[3];
+        compat_ih<false>(a, ih);
+        const Rec g = load_rec<false>(a, gid, ih);
+        const float4 x = __ldg(a.ext + gid);
+        const bool hw = __fsub_rn(g.c1, x.y) <= float(h0 + 7) && __fadd_rn(g.c1, x.y) >= float(h0) &&
+                        __fsub_rn(g.c2, x.z) <= float(w0 + 7) && __fadd_rn(g.c2, x.z) >= float(w0);
+        const float lo = __fsub_rn(g.c0, x.x), hi = __fadd_rn(g.c0, x.x);
+        const float e1 = __fsub_rn(ev1, g.c1);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int ds = d0 + 4 * r;
+            const bool kept = !a.cull || (hw && lo <= float(ds + 3) && hi >= float(ds));
+            const int gd = ds + (lane >> 3);
+            const float e0 = __fsub_rn(float(gd), g.c0);
+            const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
+            bool slot_any = false;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float m = row_m(g.q22, A, B, __fsub_rn(float(w0 + k), g.c2));
+                const bool in = m <= kCut;
+                c_inc += (in && gd < a.d && h_ok && w0 + k < a.w) ? 1 : 0;
+                const bool col = __any_sync(kFull, in);
+                slot_any |= col;
+                if (kept && col && lane == 0) c_lanes += 32;
+            }
+            if (kept) {
+                c_eval += 8;
+                if (!slot_any && lane == 0) c_empty += 1;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c_inc += __shfl_xor_sync(kFull, c_inc, o);
+        c_eval += __shfl_xor_sync(kFull, c_eval, o);
+        c_lanes += __shfl_xor_sync(kFull, c_lanes, o);
+        c_empty += __shfl_xor_sync(kFull, c_empty, o);
+    }
+    if (lane == 0) {
+        atomicAdd(out, c_inc);
+        atomicAdd(out + 1, c_eval);
+        atomicAdd(out + 2, c_lanes);
+        atomicAdd(out + 3, c_empty);
+    }
+}
+
 int grid_for(int64_t items, int block) {
     int64_t g = (items + block - 1) / block;
     return int(g < 1 ? 1 : g);
@@ -1308,6 +1379,30 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
         GSV_LAUNCH_CHECK();
     }
     k_finalize<<<grid_for(n, 256), 256, 0, st>>>(a);
+    GSV_LAUNCH_CHECK();
+    return GSV_OK;
+}
+
+int gsv_count_work(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs, int64_t capacity,
+                   const gsv_tuning* tuning, unsigned long long* out, void* stream) {
+    if (!tuning_ok(tuning) || shape.tile_size != 8 || !out) return GSV_ERR_INVALID_ARGUMENT;
+    GaussLayout G;
+    PairLayout P;
+    int64_t ntiles = 0;
+    if (layout_for(shape, n, capacity, 0, &G, &P, &ntiles) != GSV_OK || !ws_gauss || (capacity > 0 && !ws_pairs))
+        return GSV_ERR_INVALID_ARGUMENT;
+    if (ntiles > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GSV_CUDA_TRY(cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), st));
+    if (capacity == 0 || n == 0) return GSV_OK;
+    RenderArgs a{};
+    fill_shape(a, shape);
+    a.recs = cat<Rec>(ws_gauss, G.rec);
+    a.ext = cat<float4>(ws_gauss, G.ext);
+    a.ranges = cat<int2>(ws_gauss, G.ranges);
+    a.pair_ids = cat<int32_t>(ws_pairs, P.vals_out);
+    if (tuning) a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
+    k_count_work<<<unsigned(ntiles), kThreads, 0, st>>>(a, out);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }

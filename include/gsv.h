@@ -213,6 +213,20 @@ GSV_API int gsv_backward_ex(const gsv_params* params, gsv_shape shape, void* ws_
                             int64_t capacity, const float* grad_volume, const gsv_grads* grads, int flags,
                             const gsv_tuning* tuning, void* stream);
 
+/* No counterpart in the reference: a census of the work the tile-8 render
+ * kernels do on a binned problem (a diagnostic for the roofline; results
+ * unchanged).  out: FOUR device uint64 counters, overwritten --
+ *   [0] included candidates (Mahalanobis <= 9, voxel inside the volume),
+ *   [1] candidates the kernels evaluate the quadratic for (voxels of the
+ *       4x8x8 row slots the extent cull keeps),
+ *   [2] lanes issued by the per-column exp / FMA blocks (32 per voxel column
+ *       of a kept slot in which some lane is inside the cutoff),
+ *   [3] kept slots without any included voxel.
+ * tuning (may be NULL): only GSV_TUNE_NO_CULL is read.  Tile edge 8 only.
+ * Asynchronous on `stream`. */
+GSV_API int gsv_count_work(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,
+                           int64_t capacity, const gsv_tuning* tuning, unsigned long long* out, void* stream);
+
 /* ---- reference-compatible binning ------------------------------------ */
 
 /* build_tile_pairs(center_vox [n,3], radius_vox [n]) part 1: box + count +
@@ -239,9 +253,8 @@ GSV_API int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss
  * GSV_ERR_CAPACITY; GSV_ERR_CAPACITY also when the pair total exceeds
  * `pair_capacity`).  `*total_pairs` always receives the pair total; the call
  * synchronises `stream` once to read it.  The first call on a device (with
- * that device current) looks up the array's device address; make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race, so serialise them. */
+ * that device current) looks up the array's device address.  All calls share the array: calls that overlap on
+ * the GPU race, so serialise them. */
 GSV_API int gsv_build_tile_pairs_noalloc(const float* center_vox, const float* radius_vox, int64_t n,
                                          gsv_shape shape, int32_t* tile_ranges, int32_t* pair_ids,
                                          int64_t pair_capacity, int64_t* total_pairs, void* stream);

@@ -4,6 +4,10 @@ reference-kernel timing), never part of the product.
 
     python oracle/build_ref.py [--reference /path/to/GS_TMI]
 
+The reference checkout is taken from --reference, else from the
+GSV_REFERENCE_ROOT environment variable, else from DEFAULT_REFERENCE (where
+this build's recipe finds it).
+
 Sources (read in place, never copied):
     3DGS/3dgsVC/gaussian/cuda_ext/tile_voxelize_cuda.cpp
     3DGS/3dgsVC/gaussian/cuda_ext/tile_voxelize_cuda_kernel.cu
@@ -29,13 +33,20 @@ MODULE = "tile_voxelize_cuda_ref"
 SO = os.path.join(OUT, MODULE + ".so")
 
 
+DEFAULT_REFERENCE = "/root/reference"
+
+
+def reference_root(reference: str | None = None) -> str:
+    return reference or os.environ.get("GSV_REFERENCE_ROOT") or DEFAULT_REFERENCE
+
+
 def sources(reference: str):
     base = os.path.join(reference, "3DGS", "3dgsVC", "gaussian", "cuda_ext")
     return (os.path.join(base, "tile_voxelize_cuda.cpp"), os.path.join(base, "tile_voxelize_cuda_kernel.cu"))
 
 
-def build(reference: str = "/root/reference", force: bool = False) -> str | None:
-    cpp, cu = sources(reference)
+def build(reference: str | None = None, force: bool = False) -> str | None:
+    cpp, cu = sources(reference_root(reference))
     if not (os.path.exists(cpp) and os.path.exists(cu)):
         return SO if os.path.exists(SO) else None
     if not force and os.path.exists(SO) and os.path.getmtime(SO) >= max(os.path.getmtime(cpp), os.path.getmtime(cu)):
@@ -78,7 +89,8 @@ def load():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None, help="reference checkout (default: $GSV_REFERENCE_ROOT, "
+                                                         "else DEFAULT_REFERENCE)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     out = build(a.reference, a.force)

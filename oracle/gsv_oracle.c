@@ -68,7 +68,7 @@ static float nanmax3(float a, float b, float c) {
  * M = T T^T with T = R(q / (|q| + 1e-8)) diag(1 / (s + 1e-8))
  * (tile_voxelizer.py:77-84, :287-290).  Op order is the kernel's.
  */
-static void qcoef_f32(const float* s, const float* q, const float* ih, float* out) {
+static void rot_f32(const float* q, float* r) {
     float n2 = q[0] * q[0];
     n2 = n2 + q[1] * q[1];
     n2 = n2 + q[2] * q[2];
@@ -76,7 +76,6 @@ static void qcoef_f32(const float* s, const float* q, const float* ih, float* ou
     float den = sqrtf(n2) + 1e-8f;
     float w = q[0] / den, x = q[1] / den, y = q[2] / den, z = q[3] / den;
     float tx = 2.0f * x, ty = 2.0f * y, tz = 2.0f * z;
-    float r[9];
     r[0] = (1.0f - ty * y) - tz * z;
     r[1] = tx * y - tz * w;
     r[2] = tx * z + ty * w;
@@ -86,6 +85,11 @@ static void qcoef_f32(const float* s, const float* q, const float* ih, float* ou
     r[6] = tx * z - ty * w;
     r[7] = ty * z + tx * w;
     r[8] = (1.0f - tx * x) - ty * y;
+}
+
+static void qcoef_f32(const float* s, const float* q, const float* ih, float* out) {
+    float r[9];
+    rot_f32(q, r);
     float si[3];
     for (int j = 0; j < 3; ++j) si[j] = 1.0f / (s[j] + 1e-8f);
     float t[9];
@@ -124,6 +128,70 @@ static int included_f32(const float* qc, float e0, float e1, float e2) {
     float b = fmaf(qc[4], e1, qc[2] * e0);
     float m = fmaf(fmaf(qc[5], e2, b), e2, a);
     return m <= 9.0f;
+}
+
+/* ------------------------------------------------------------------ */
+/* The reference's own FP32 op order for the inclusion test.           */
+/*                                                                      */
+/* tile_voxelize_cuda_kernel.cu:118-130 evaluates, per voxel v and      */
+/* Gaussian (c, M):                                                     */
+/*   dx = (v0 - c0) / hs0  (dy, dz alike)                               */
+/*   md_a = M_a0 dx + M_a1 dy + M_a2 dz                                 */
+/*   mahal = dx md_0 + dy md_1 + dz md_2,  included iff mahal <= 9      */
+/* in FP32 with nvcc's default contraction of a left-to-right sum of    */
+/* products: the first product rounded, each later one fused,           */
+/* fma(x2, y2, fma(x1, y1, x0 * y0)).  The extension is built with       */
+/* --use_fast_math (tile_voxelizer.py:58-66), whose division is          */
+/* approximate; ORC_PRED_REFERENCE_RCP models it as a product with the   */
+/* correctly rounded reciprocal.  Both agree with IEEE division when hs  */
+/* is a power of two.  M is the FP32 cov_inv the reference passes in:   */
+/* in the compat layout the caller's array; in the params layout         */
+/* T T^T with T = R(q) diag(1 / (s + 1e-8)) (tile_voxelizer.py:287-290)  */
+/* accumulated with FMAs, as a batched GEMM does.                        */
+/* ------------------------------------------------------------------ */
+
+enum { ORC_PRED_ROWFORM = 0, ORC_PRED_REFERENCE = 1, ORC_PRED_REFERENCE_RCP = 2 };
+static int g_pred = ORC_PRED_ROWFORM;
+
+/* Selects the inclusion test of orc_forward / orc_backward; returns the
+ * previous mode.  Not thread-safe: oracle.py serialises its callers. */
+ORC_EXPORT int orc_set_predicate(int mode) {
+    int old = g_pred;
+    g_pred = (mode == ORC_PRED_REFERENCE || mode == ORC_PRED_REFERENCE_RCP) ? mode : ORC_PRED_ROWFORM;
+    return old;
+}
+
+static void refcov_f32(const float* s, const float* q, float* m9) {
+    float r[9], si[3], t[9];
+    rot_f32(q, r);
+    for (int j = 0; j < 3; ++j) si[j] = 1.0f / (s[j] + 1e-8f);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i * 3 + j] = r[i * 3 + j] * si[j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const float* ta = &t[i * 3];
+            const float* tb = &t[j * 3];
+            m9[i * 3 + j] = fmaf(ta[2], tb[2], fmaf(ta[1], tb[1], ta[0] * tb[0]));
+        }
+}
+
+static int included_ref_f32(int mode, const float* c, const float* m, const float* hs, float v0, float v1,
+                            float v2) {
+    float dx, dy, dz;
+    if (mode == ORC_PRED_REFERENCE_RCP) {
+        dx = (v0 - c[0]) * (1.0f / hs[0]);
+        dy = (v1 - c[1]) * (1.0f / hs[1]);
+        dz = (v2 - c[2]) * (1.0f / hs[2]);
+    } else {
+        dx = (v0 - c[0]) / hs[0];
+        dy = (v1 - c[1]) / hs[1];
+        dz = (v2 - c[2]) / hs[2];
+    }
+    float md0 = fmaf(m[2], dz, fmaf(m[1], dy, m[0] * dx));
+    float md1 = fmaf(m[5], dz, fmaf(m[4], dy, m[3] * dx));
+    float md2 = fmaf(m[8], dz, fmaf(m[7], dy, m[6] * dx));
+    float mahal = fmaf(dz, md2, fmaf(dy, md1, dx * md0));
+    return mahal <= 9.0f;
 }
 
 /* ------------------------------------------------------------------ */
@@ -385,6 +453,46 @@ static void build_state(int compat, int64_t n, const shape_t* sh, const float* a
     }
 }
 
+/* FP32 inputs of one inclusion test, in either op order. */
+typedef struct {
+    int mode;           /* ORC_PRED_* */
+    const float* cen;   /* [n,3] center_vox */
+    const float* qc;    /* [n,6] row-form coefficients (ORC_PRED_ROWFORM) */
+    const float* m9;    /* [n,9] FP32 cov_inv (reference op orders) */
+    float hs[3];        /* FP32 half shape (reference op orders) */
+} pred_t;
+
+/* m9 (may be NULL when mode is the row form): the reference's FP32 cov_inv. */
+static void build_pred(int mode, int compat, int64_t n, const shape_t* sh, const float* b32,
+                       const float* c32, const float* hs32, const float* cen32, const float* qc32,
+                       float* m9, pred_t* P) {
+    P->mode = mode;
+    P->cen = cen32;
+    P->qc = qc32;
+    P->m9 = NULL;
+    if (compat) {
+        for (int a = 0; a < 3; ++a) P->hs[a] = hs32[a];
+    } else {
+        P->hs[0] = (float)sh->d * 0.5f;
+        P->hs[1] = (float)sh->h * 0.5f;
+        P->hs[2] = (float)sh->w * 0.5f;
+    }
+    if (mode == ORC_PRED_ROWFORM) return;
+    if (compat) {
+        P->m9 = b32;
+    } else {
+        for (int64_t g = 0; g < n; ++g) refcov_f32(&b32[g * 3], &c32[g * 4], &m9[g * 9]);
+        P->m9 = m9;
+    }
+}
+
+static int pred_incl(const pred_t* P, int32_t g, int32_t i, int32_t j, int32_t k) {
+    const float* c = &P->cen[(int64_t)g * 3];
+    if (P->mode == ORC_PRED_ROWFORM)
+        return included_f32(&P->qc[(int64_t)g * 6], (float)i - c[0], (float)j - c[1], (float)k - c[2]);
+    return included_ref_f32(P->mode, c, &P->m9[(int64_t)g * 9], P->hs, (float)i, (float)j, (float)k);
+}
+
 static void tile_origin(const shape_t* sh, int64_t t, int32_t* o) {
     int64_t per = (int64_t)sh->nth * sh->ntw;
     int32_t td = (int32_t)(t / per);
@@ -428,6 +536,10 @@ ORC_EXPORT int orc_forward(int compat, const float* a32, const float* b32, const
     g64_t* g64 = (g64_t*)malloc((size_t)(n ? n : 1) * sizeof(g64_t));
     build_state(compat, n, &sh, a32, b32, c32, dr32, di32, hs32, a64, b64, c64, dr64, di64, cen32, qc32,
                 g64);
+    float* m9 = (g_pred != ORC_PRED_ROWFORM && !compat) ? (float*)malloc((size_t)(n ? n : 1) * 9 * sizeof(float))
+                                                         : NULL;
+    pred_t P;
+    build_pred(g_pred, compat, n, &sh, b32, c32, hs32, cen32, qc32, m9, &P);
     double hs[3];
     half_shape64(compat, &sh, hs32, hs);
     memset(vol, 0, (size_t)d * h * w * 2 * sizeof(double));
@@ -445,10 +557,8 @@ ORC_EXPORT int orc_forward(int compat, const float* a32, const float* b32, const
                     double v[3] = {i, j, k};
                     for (int32_t p = s0; p < s1; ++p) {
                         int32_t g = pair_ids[p];
-                        const float* c = &cen32[g * 3];
                         ++cand;
-                        if (!included_f32(&qc32[g * 6], (float)i - c[0], (float)j - c[1], (float)k - c[2]))
-                            continue;
+                        if (!pred_incl(&P, g, i, j, k)) continue;
                         ++incl;
                         double dn[3], md[3];
                         double wgt = eval64(&g64[g], v, hs, dn, md);
@@ -464,6 +574,7 @@ ORC_EXPORT int orc_forward(int compat, const float* a32, const float* b32, const
         stats[0] = cand;
         stats[1] = incl;
     }
+    free(m9);
     free(cen32);
     free(qc32);
     free(g64);
@@ -491,6 +602,9 @@ ORC_EXPORT int orc_backward(int compat, const float* a32, const float* b32, cons
     g64_t* g64 = (g64_t*)malloc((size_t)nn * sizeof(g64_t));
     build_state(compat, n, &sh, a32, b32, c32, dr32, di32, hs32, a64, b64, c64, dr64, di64, cen32, qc32,
                 g64);
+    float* m9 = (g_pred != ORC_PRED_ROWFORM && !compat) ? (float*)malloc((size_t)nn * 9 * sizeof(float)) : NULL;
+    pred_t P;
+    build_pred(g_pred, compat, n, &sh, b32, c32, hs32, cen32, qc32, m9, &P);
     double hs[3];
     half_shape64(compat, &sh, hs32, hs);
     double* part = (double*)calloc((size_t)(n_pairs ? n_pairs : 1) * NMOM, sizeof(double));
@@ -502,14 +616,12 @@ ORC_EXPORT int orc_backward(int compat, const float* a32, const float* b32, cons
         tile_origin(&sh, t, o);
         for (int32_t p = s0; p < s1; ++p) {
             int32_t g = pair_ids[p];
-            const float* c = &cen32[g * 3];
             const g64_t* G = &g64[g];
             double* mo = &part[(int64_t)p * NMOM];
             for (int32_t i = o[0]; i < o[0] + ts && i < d; ++i)
                 for (int32_t j = o[1]; j < o[1] + ts && j < h; ++j)
                     for (int32_t k = o[2]; k < o[2] + ts && k < w; ++k) {
-                        if (!included_f32(&qc32[g * 6], (float)i - c[0], (float)j - c[1], (float)k - c[2]))
-                            continue;
+                        if (!pred_incl(&P, g, i, j, k)) continue;
                         int64_t f = ((int64_t)i * h + j) * w + k;
                         double gvr = grad_vol[f * 2], gvi = grad_vol[f * 2 + 1];
                         double v[3] = {i, j, k}, dn[3], md[3];
@@ -542,6 +654,7 @@ ORC_EXPORT int orc_backward(int compat, const float* a32, const float* b32, cons
     }
     free(tot);
     free(part);
+    free(m9);
     free(cen32);
     free(qc32);
     free(g64);
@@ -561,6 +674,62 @@ ORC_EXPORT int64_t orc_candidate_evals(const int32_t* tile_ranges, int32_t d, in
         e += (int64_t)(tile_ranges[t * 2 + 1] - tile_ranges[t * 2]) * nv;
     }
     return e;
+}
+
+/* Listed (voxel, Gaussian) candidates on which two inclusion tests
+ * disagree.  out[0]: included by both, out[1]: by mode_a only, out[2]: by
+ * mode_b only, out[3]: candidates.  vflags (may be NULL, [d*h*w]): set to 1
+ * at every voxel with a disagreement.  Inputs as orc_forward's FP32 ones. */
+ORC_EXPORT int orc_predicate_flips(int compat, const float* a32, const float* b32, const float* c32,
+                                   const float* hs32, int64_t n, int32_t d, int32_t h, int32_t w, int32_t ts,
+                                   const int32_t* tile_ranges, const int32_t* pair_ids, int mode_a, int mode_b,
+                                   int64_t* out, uint8_t* vflags) {
+    shape_t sh = mkshape(d, h, w, ts);
+    int64_t nn = n ? n : 1;
+    float* cen32 = (float*)malloc((size_t)nn * 3 * sizeof(float));
+    float* qc32 = (float*)malloc((size_t)nn * 6 * sizeof(float));
+    float* m9 = compat ? NULL : (float*)malloc((size_t)nn * 9 * sizeof(float));
+    if (compat) {
+        memcpy(cen32, a32, (size_t)n * 3 * sizeof(float));
+        orc_qcoef_from_covinv_f32(b32, hs32, n, qc32);
+    } else {
+        orc_preprocess_f32(a32, b32, c32, n, d, h, w, cen32, NULL, qc32);
+    }
+    pred_t PA, PB;
+    build_pred(mode_a, compat, n, &sh, b32, c32, hs32, cen32, qc32, m9, &PA);
+    build_pred(mode_b, compat, n, &sh, b32, c32, hs32, cen32, qc32, m9, &PB);
+    if (vflags) memset(vflags, 0, (size_t)d * h * w);
+    int64_t both = 0, a_only = 0, b_only = 0, cand = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : both, a_only, b_only, cand)
+    for (int64_t t = 0; t < sh.ntiles; ++t) {
+        int32_t s0 = tile_ranges[t * 2], s1 = tile_ranges[t * 2 + 1];
+        if (s0 >= s1) continue;
+        int32_t o[3];
+        tile_origin(&sh, t, o);
+        for (int32_t i = o[0]; i < o[0] + ts && i < d; ++i)
+            for (int32_t j = o[1]; j < o[1] + ts && j < h; ++j)
+                for (int32_t k = o[2]; k < o[2] + ts && k < w; ++k) {
+                    int flip = 0;
+                    for (int32_t p = s0; p < s1; ++p) {
+                        int32_t g = pair_ids[p];
+                        int ia = pred_incl(&PA, g, i, j, k), ib = pred_incl(&PB, g, i, j, k);
+                        ++cand;
+                        both += ia && ib;
+                        a_only += ia && !ib;
+                        b_only += ib && !ia;
+                        flip |= ia != ib;
+                    }
+                    if (flip && vflags) vflags[((int64_t)i * h + j) * w + k] = 1;
+                }
+    }
+    out[0] = both;
+    out[1] = a_only;
+    out[2] = b_only;
+    out[3] = cand;
+    free(m9);
+    free(cen32);
+    free(qc32);
+    return 0;
 }
 
 ORC_EXPORT int orc_num_threads(void) {

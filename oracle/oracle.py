@@ -81,10 +81,32 @@ def lib():
             L.orc_poisson_mask.argtypes = [_f64p, _i32p, _i32, _i32, _i32, _i64,
                                            np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")]
             L.orc_poisson_mask.restype = _i64
+            L.orc_set_predicate.argtypes = [ctypes.c_int]
+            L.orc_set_predicate.restype = ctypes.c_int
+            L.orc_predicate_flips.argtypes = [ctypes.c_int, _vp, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _i32,
+                                              _i32p, _i32p, ctypes.c_int, ctypes.c_int,
+                                              np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS"), _vp]
+            L.orc_predicate_flips.restype = ctypes.c_int
             L.orc_num_threads.argtypes = []
             L.orc_num_threads.restype = ctypes.c_int
             _lib = L
     return _lib
+
+
+# Inclusion tests the oracle can evaluate (gsv_oracle.c, ORC_PRED_*):
+ROWFORM = 0        # the kernels' voxel-unit row form, shared bit for bit
+REFERENCE = 1      # the reference CUDA kernel's op order, IEEE division by hs
+REFERENCE_RCP = 2  # the same with the division as a product by the reciprocal
+_pred_lock = threading.Lock()
+
+
+def _with_predicate(mode, fn):
+    with _pred_lock:
+        old = lib().orc_set_predicate(int(mode))
+        try:
+            return fn()
+        finally:
+            lib().orc_set_predicate(old)
 
 
 def _c(a, dtype):
@@ -150,13 +172,15 @@ def _args(compat, a, b, c, dr, di, hs, o64):
 
 
 def forward(params, shape, tile_size, tile_ranges, pair_ids, overrides64=None, compat=False,
-            half_shape=None):
+            half_shape=None, predicate=ROWFORM):
     """FP64 complex volume [d,h,w] and stats (candidates, included).
 
     ``params`` = (positions, scales, rotations, density_r, density_i) or, with
     ``compat=True``, (center_vox, cov_inv[n,9], None, density_r, density_i).
     ``overrides64`` maps a/b/c/dr/di to FP64 arrays used for the arithmetic
     while the FP32 ``params`` fix the inclusion predicate (finite differences).
+    ``predicate`` selects the FP32 inclusion test (ROWFORM, REFERENCE,
+    REFERENCE_RCP); everything else stays FP64.
     """
     a, b, c, dr, di = params
     n = np.asarray(dr).shape[0]
@@ -167,13 +191,14 @@ def forward(params, shape, tile_size, tile_ranges, pair_ids, overrides64=None, c
     tr, pid = _c(tile_ranges, np.int32), _c(pair_ids, np.int32)
     if pid.size == 0:
         pid = np.zeros(1, np.int32)
-    lib().orc_forward(int(compat), *ptrs, n, d, h, w, tile_size, tr, pid, vol, _ptr(stats))
+    _with_predicate(predicate, lambda: lib().orc_forward(int(compat), *ptrs, n, d, h, w, tile_size, tr, pid, vol,
+                                                        _ptr(stats)))
     del keep
     return (vol[0::2] + 1j * vol[1::2]).reshape(d, h, w), stats
 
 
 def backward(params, shape, tile_size, tile_ranges, pair_ids, grad_vol, overrides64=None,
-             compat=False, half_shape=None):
+             compat=False, half_shape=None, predicate=ROWFORM):
     """FP64 gradients.  params mode -> (d_pos[n,3], d_scale[n,3], d_rot[n,4],
     d_rho_r[n], d_rho_i[n]); compat mode -> (d_center[n,3], d_cov_inv[n,3,3],
     None, d_rho_r[n], d_rho_i[n])."""
@@ -195,8 +220,9 @@ def backward(params, shape, tile_size, tile_ranges, pair_ids, grad_vol, override
     npairs = pid.size
     if npairs == 0:
         pid = np.zeros(1, np.int32)
-    lib().orc_backward(int(compat), *ptrs, n, d, h, w, tile_size, tr, pid, npairs, gv, _ptr(o1),
-                       _ptr(o2), _ptr(o3), _ptr(o4), _ptr(o5))
+    _with_predicate(predicate, lambda: lib().orc_backward(int(compat), *ptrs, n, d, h, w, tile_size, tr, pid,
+                                                         npairs, gv, _ptr(o1), _ptr(o2), _ptr(o3), _ptr(o4),
+                                                         _ptr(o5)))
     del keep
     if compat:
         return o1[: n * 3].reshape(n, 3), o2[: n * 9].reshape(n, 3, 3), None, o4[:n], o5[:n]
@@ -236,6 +262,31 @@ def fd_gradient(params, shape, tile_size, tile_ranges, pair_ids, grad_vol, which
         return float(np.sum(vol.real * g.real + vol.imag * g.imag))
 
     return (loss(h) - loss(-h)) / (2 * h)
+
+
+def predicate_flips(params, shape, tile_size, tile_ranges, pair_ids, mode_a=ROWFORM, mode_b=REFERENCE,
+                    compat=False, half_shape=None, voxel_flags=False):
+    """Listed candidates on which two FP32 inclusion tests disagree.
+
+    Returns {"both", "a_only", "b_only", "candidates"} and, with
+    ``voxel_flags``, a boolean [d,h,w] mask of the voxels with a
+    disagreement.  ``params`` as in :func:`forward` (densities unused)."""
+    a, b, c = params[:3]
+    a, b, c = _c(a, np.float32), _c(b, np.float32), _c(c, np.float32)
+    hs = _c(half_shape, np.float32)
+    n = a.shape[0]
+    d, h, w = shape
+    out = np.zeros(4, np.int64)
+    flags = np.zeros(d * h * w, np.uint8) if voxel_flags else None
+    tr, pid = _c(tile_ranges, np.int32), _c(pair_ids, np.int32)
+    if pid.size == 0:
+        pid = np.zeros(1, np.int32)
+    lib().orc_predicate_flips(int(compat), _ptr(a), _ptr(b), _ptr(c), _ptr(hs), n, d, h, w, tile_size, tr, pid,
+                              int(mode_a), int(mode_b), out, _ptr(flags))
+    res = {"both": int(out[0]), "a_only": int(out[1]), "b_only": int(out[2]), "candidates": int(out[3])}
+    if voxel_flags:
+        return res, flags.reshape(d, h, w).astype(bool)
+    return res
 
 
 def boundary_voxels(positions, scales, rotations, shape, tile_size, tile_ranges, pair_ids, tol=1e-4):

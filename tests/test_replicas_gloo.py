@@ -49,3 +49,15 @@ def test_reference_arm_runs_on_rank0_only():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                         "--warmup", "3"], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_maps_no_product_library():
+    """The reference arm builds its seeded inputs without importing the
+    product package, so libgsv_b200.so is never mapped in its process."""
+    code = ("import sys; sys.path.insert(0, %r); import bench; "
+            "gs, gv = bench.make_inputs('cube64_n20k', standalone=True); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPPED' if 'libgsv_b200' in maps else 'CLEAN', gs.n, tuple(gv.shape))") % ROOT
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.split() == ["CLEAN", "20000", "(64,", "64,", "64)"], r.stdout

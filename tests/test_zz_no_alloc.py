@@ -23,7 +23,7 @@ import torch
 
 import gs_tmi_b200
 from gs_tmi_b200 import synthetic
-from gs_tmi_b200._lib import GSV_ERR_CAPACITY, GSV_ERR_INVALID_ARGUMENT, GSV_OK, GsvShape, lib
+from gs_tmi_b200._lib import GSV_ERR_CAPACITY, GSV_ERR_EMPTY_BOX, GSV_ERR_INVALID_ARGUMENT, GSV_OK, GsvShape, lib
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -101,3 +101,37 @@ def test_limits_are_refused(cuda_device):
     rc, total, _, _ = _noalloc(torch.tensor(c, device=cuda_device), torch.tensor(r, device=cuda_device),
                                shape, ts, capacity=10)
     assert rc == GSV_ERR_CAPACITY and total > 10
+
+
+def test_negative_radius_is_refused_and_the_next_call_is_clean(cuda_device):
+    """A negative radius gives an empty tile box, which the reference's
+    binning cannot handle either: the call returns GSV_ERR_EMPTY_BOX.  The
+    flag lives in the shared array, so the following valid call must still
+    match the regular binning."""
+    shape, ts, c, r = _case("ragged_ts8")
+    r_bad = r.copy()
+    r_bad[5] = -50.0
+    rc, _, _, _ = _noalloc(torch.tensor(c, device=cuda_device), torch.tensor(r_bad, device=cuda_device), shape, ts,
+                           capacity=1 << 20)
+    assert rc == GSV_ERR_EMPTY_BOX
+    center, radius = torch.tensor(c, device=cuda_device), torch.tensor(r, device=cuda_device)
+    ref_tr, ref_pid = gs_tmi_b200.build_tile_pairs(center, radius, shape, ts)
+    rc, total, tr, pid = _noalloc(center, radius, shape, ts, capacity=ref_pid.numel())
+    assert rc == GSV_OK and total == ref_pid.numel()
+    assert np.array_equal(tr, ref_tr.cpu().numpy()) and np.array_equal(pid[:total], ref_pid.cpu().numpy())
+
+
+def test_one_large_gaussian_is_spread_over_the_warp(cuda_device):
+    """A single Gaussian whose box covers every tile of a 256^3 volume at
+    tile edge 4 (262,144 pairs) next to small ones: the pairs of the large
+    one are emitted by the whole warp, in the reference's raster order."""
+    shape, ts = (256, 256, 256), 4
+    gs = synthetic.random_gaussians(40, shape, seed=91)
+    c, r, _ = O.preprocess_f32(gs.positions.numpy(), gs.scales.numpy(), gs.rotations.numpy(), shape)
+    c[7] = 127.5
+    r[7] = 400.0
+    center, radius = torch.tensor(c, device=cuda_device), torch.tensor(r, device=cuda_device)
+    ref_tr, ref_pid = gs_tmi_b200.build_tile_pairs(center, radius, shape, ts)
+    rc, total, tr, pid = _noalloc(center, radius, shape, ts, capacity=ref_pid.numel())
+    assert rc == GSV_OK and total == ref_pid.numel() >= 64 ** 3
+    assert np.array_equal(tr, ref_tr.cpu().numpy()) and np.array_equal(pid[:total], ref_pid.cpu().numpy())
