@@ -499,6 +499,42 @@ class Workload:
         self.fwd()
         self.bwd()
 
+    def capture(self):
+        """The whole step as one CUDA graph: binning writes into the fixed
+        pair capacity and nothing in the step synchronises the host, so it
+        replays without CPU launch overhead."""
+        dev = self.dev
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            self.step()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        torch.cuda.synchronize(dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self.step()
+        torch.cuda.synchronize(dev)
+        return g
+
+    def time_graph(self, graph, steps, warmup, flush):
+        """Per-step device time (ms) of graph replays, L2 flushed between."""
+        dev = self.dev
+        for _ in range(warmup):
+            graph.replay()
+        torch.cuda.synchronize(dev)
+        cur = torch.cuda.current_stream(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(cur)
+            graph.replay()
+            ev[i][1].record(cur)
+        torch.cuda.synchronize(dev)
+        _, fl = self.plan.read_status(torch_stream(dev))
+        if fl:
+            raise RuntimeError(f"voxelizer status flags {fl} during the timed region")
+        return [a.elapsed_time(b) for a, b in ev]
+
     def time(self, steps, warmup, flush, dist=None):
         """Per-step device times (ms) of binning, forward and backward, CUDA
         events on the launching stream, L2 flushed between steps."""
@@ -569,6 +605,7 @@ def roofline_of(wl, t, peak_ops, pk, pk_kind, sm_mhz):
             "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
             "work": {"candidates": wl.evals, "included": useful, "evaluated_after_cull": c["evaluated"],
                      "exp_block_lanes": c["exp_block_lanes"], "empty_kept_slots": c["empty_kept_slots"],
+                     "row_min_passed_slots": c["row_min_passed_slots"],
                      "lane_efficiency": useful / max(c["exp_block_lanes"], 1)},
             "pipes_ncu": pipes,
             "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9, "peak_gbs": pk.get("hbm_gbs")}}
@@ -653,9 +690,20 @@ def run_ours(args, rank, world, dist):
     torch.cuda.synchronize(dev)
     n_launch, kernel_names = (None, []) if args.no_launch_count else count_library_launches(wl.step, dev)
 
+    graph = None if args.eager else wl.capture()
     with ClockSampler(local) as clk:
+        # per-phase breakdown from eagerly launched steps; the headline from graph replays of the
+        # same step (the launch mode of the graph-captured reconstruction loops) unless --eager
         t = wl.time(args.steps, args.warmup, flush, dist)
-        total_ms = sum(t["step"])
+        eager_ms = sum(t["step"])
+        if graph is not None:
+            if dist:
+                dist.barrier()
+            total_ms = sum(wl.time_graph(graph, args.steps, args.warmup, flush))
+            if dist:
+                dist.barrier()
+        else:
+            total_ms = eager_ms
 
         # e2e through the public module with pinned host buffers
         vox = TileVoxelizer(shape, tile_size=TILE, device=str(dev), deterministic=args.deterministic,
@@ -702,16 +750,19 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize(dev)
         e2e_ms = e0.elapsed_time(e1)
 
-        total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], dist, dev)
+        total_ms, e2e_ms, eager_ms = max_over_ranks([total_ms, e2e_ms, eager_ms], dist, dev)
         extra = {}
         if rank == 0 and world == 1 and not args.no_extras:
             # the BASELINE voxelizer micro-benchmark (64^3, N = 20,000) on the same box
             if name != "cube64_n20k":
                 small = Workload("cube64_n20k", dev, args, flags)
                 ts_ = small.time(args.steps, args.warmup, flush)
+                small_ms = sum(ts_["step"]) if args.eager else sum(
+                    small.time_graph(small.capture(), args.steps, args.warmup, flush))
                 extra["cube64_n20k"] = {
-                    "value": small.evals * args.steps / (sum(ts_["step"]) * 1e-3) / 1e9, "unit": "Gvox-evals/s",
-                    "ms_per_step": sum(ts_["step"]) / args.steps, "evals_per_step": small.evals,
+                    "value": small.evals * args.steps / (small_ms * 1e-3) / 1e9, "unit": "Gvox-evals/s",
+                    "ms_per_step": small_ms / args.steps, "eager_ms_per_step": sum(ts_["step"]) / args.steps,
+                    "evals_per_step": small.evals,
                     "breakdown_ms": {"prepare_bin": statistics.mean(ts_["bin"]),
                                      "forward": statistics.mean(ts_["fwd"]),
                                      "backward": statistics.mean(ts_["bwd"])},
@@ -733,9 +784,12 @@ def run_ours(args, rank, world, dist):
         "config": {"workload": name, "volume": list(shape), "gaussians": n, "tile_size": TILE, "pairs": wl.total,
                    "evals_per_step": evals, "deterministic": bool(args.deterministic),
                    "execution": wl.execution(),
+                   "launch": "eager" if graph is None else "one CUDA graph per step (preprocess, binning, "
+                                                           "forward, backward)",
                    "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
+        "eager_ms_per_step": eager_ms / args.steps,
         "breakdown_ms": {"prepare_bin": statistics.mean(t["bin"]), "forward": statistics.mean(t["fwd"]),
-                         "backward": statistics.mean(t["bwd"])},
+                         "backward": statistics.mean(t["bwd"]), "launch": "eager"},
         "roofline": roofline_of(wl, t, peak_ops, pk, pk_kind, sm_mhz),
         "e2e": {"value": whole_job_rate(evals, args.steps, world, e2e_ms) / 1e9, "unit": "Gvox-evals/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms / args.steps,
@@ -762,6 +816,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the CUDA activity trace (under ncu)")
     ap.add_argument("--no-autotune", action="store_true", help="default execution shape, no tuning pass")
+    ap.add_argument("--eager", action="store_true", help="time eagerly launched steps instead of graph replays")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the 64^3 line and the reference-CUDA baseline (under ncu)")
     args = ap.parse_args()

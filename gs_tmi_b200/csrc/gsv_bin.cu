@@ -234,17 +234,31 @@ __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ 
 // Gaussian a pair belongs to by a 5-step search over the warp's 32 offsets
 // (coalesced, balanced however the pair counts are spread).  Tiles follow
 // the (d,h,w) raster order of each Gaussian's tile box.
+// Emission of the pairs in Gaussian-major (d,h,w) raster order
+// (tile_voxelizer.py:126-145), plus the two fills the sort and the range
+// pass need: the tile ranges cleared to (0,0) and the sort padding past the
+// pair total (keys = ntiles, after every real tile) -- one launch.
+// A warp owns 32 consecutive Gaussians and writes their pairs as one
+// contiguous range: lane l takes pairs base + l, base + 32 + l, ... and finds
+// its Gaussian by a shuffle binary search over the warp's first indices.
 __global__ void __launch_bounds__(128) k_emit(const int4* __restrict__ boxes,
                                               const int64_t* __restrict__ offsets, int64_t n,
                                               DevShape s, int64_t cap, int32_t* __restrict__ keys,
-                                              int32_t* __restrict__ vals, Status* status) {
+                                              int32_t* __restrict__ vals, int2* __restrict__ ranges,
+                                              int64_t ntiles, Status* status) {
     constexpr unsigned kAll = 0xffffffffu;
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     const int lane = threadIdx.x & 31;
+    const int64_t total = offsets[n];
     if (g == 0) {
-        const int64_t total = offsets[n];
         if (total > cap) atomicOr(&status->flags, GSV_FLAG_CAPACITY_OVERFLOW);
         if (total > int64_t(INT32_MAX)) atomicOr(&status->flags, GSV_FLAG_TOO_MANY_PAIRS);
+    }
+    for (int64_t t = g; t < ntiles; t += stride) ranges[t] = make_int2(0, 0);
+    for (int64_t i = total + g; i < cap; i += stride) {
+        keys[i] = int32_t(ntiles);
+        vals[i] = 0;
     }
     const int64_t g0 = g - lane;  // first Gaussian of this warp (warp-uniform)
     if (g0 >= n) return;
@@ -275,17 +289,6 @@ __global__ void __launch_bounds__(128) k_emit(const int4* __restrict__ boxes,
         const int32_t jj = r % n1, i = r / n1;
         keys[p] = ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
         vals[p] = int32_t(g0 + j);
-    }
-}
-
-__global__ void k_fill_sentinel(const int64_t* __restrict__ offsets, int64_t n, int64_t cap,
-                                int32_t sentinel, int32_t* __restrict__ keys,
-                                int32_t* __restrict__ vals) {
-    const int64_t total = offsets[n];
-    for (int64_t i = total + int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < cap;
-         i += int64_t(gridDim.x) * blockDim.x) {
-        keys[i] = sentinel;
-        vals[i] = 0;
     }
 }
 
@@ -332,13 +335,16 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
     int32_t* keys_out = at<int32_t>(ws_pairs, P.keys_out);
     int32_t* vals_out = vals_out_override ? vals_out_override : at<int32_t>(ws_pairs, P.vals_out);
     int2* ranges = at<int2>(ws_gauss, G.ranges);
-    GSV_CUDA_TRY(cudaMemsetAsync(ranges, 0, size_t(si.ntiles) * sizeof(int2), st));
-    if (cap == 0) return GSV_OK;
-    k_emit<<<grid_for(n, 128), 128, 0, st>>>(at<int4>(ws_gauss, G.box), offsets, n, s, cap, keys_in,
-                                             vals_in, status);
-    GSV_LAUNCH_CHECK();
-    k_fill_sentinel<<<grid_for(cap, 256) < 1184 ? grid_for(cap, 256) : 1184, 256, 0, st>>>(
-        offsets, n, cap, int32_t(si.ntiles), keys_in, vals_in);
+    if (cap == 0) {
+        GSV_CUDA_TRY(cudaMemsetAsync(ranges, 0, size_t(si.ntiles) * sizeof(int2), st));
+        return GSV_OK;
+    }
+    // enough CTAs for the emission (one thread per Gaussian) and for the fills
+    const int fill_grid = grid_for(cap > si.ntiles ? cap : si.ntiles, 128);
+    const int emit_grid = grid_for(n, 128);
+    const int grid = emit_grid > (fill_grid < 1184 ? fill_grid : 1184) ? emit_grid : (fill_grid < 1184 ? fill_grid : 1184);
+    k_emit<<<grid, 128, 0, st>>>(at<int4>(ws_gauss, G.box), offsets, n, s, cap, keys_in, vals_in, ranges,
+                                 si.ntiles, status);
     GSV_LAUNCH_CHECK();
     size_t sort_bytes = P.sort_tmp_bytes;
     GSV_CUDA_TRY(cub::DeviceRadixSort::SortPairs(at<void>(ws_pairs, P.sort_tmp), sort_bytes, keys_in,

@@ -63,6 +63,41 @@ class FitConfig:
     seed: int = 0
     capturable_adam: bool = False  # device-side LR/bias correction (what fit_graph uses)
     fused_sense: bool = True       # data term through the fused SENSE kernels (sense_data_term)
+    # the reference trainer's early stop on ground-truth metrics (PlateauStop; V/configs/default.yaml
+    # `stopping`: enable_metric_plateau, min_iterations_before_stop, patience_evals, metric_min_delta)
+    plateau_stop: bool = False
+    plateau_patience: int = 4
+    plateau_min_iterations: int = 200
+    plateau_min_delta_psnr: float = 0.05
+    plateau_min_delta_ssim: float = 0.0005
+    keep_best: bool = False  # snapshot the parameters at the best-PSNR evaluation (the reference's best.pth)
+
+
+@dataclass
+class PlateauStop:
+    """The reference trainer's early stop on ground-truth metrics
+    (V/metrics/metrics.py:166-195, driven by V/trainers/trainer.py:571-590).
+    After each evaluation a metric counts as improved when it beats its best
+    so far by more than its minimum delta; any improved metric resets the
+    count of evaluations without improvement, and the fit stops once the
+    iteration is at least `min_iterations` and `patience` evaluations in a
+    row improved nothing."""
+    patience: int = 4
+    min_iterations: int = 200
+    min_delta: Dict[str, float] = field(default_factory=lambda: {"psnr": 0.05, "ssim": 0.0005})
+    best: Dict[str, float] = field(default_factory=dict)
+    bad: int = 0
+
+    def update(self, iteration: int, metrics: Dict[str, float]) -> bool:
+        improved = False
+        for name, value in metrics.items():
+            if value is None:
+                continue
+            if name not in self.best or value > self.best[name] + self.min_delta.get(name, 0.0):
+                self.best[name] = value
+                improved = True
+        self.bad = 0 if improved else self.bad + 1
+        return iteration >= self.min_iterations and self.bad >= self.patience
 
 
 # ---------------------------------------------------------------------------
@@ -372,6 +407,10 @@ class FitResult:
     final_nmse: float = float("nan")
     final_ssim: float = float("nan")
     final_psnr: float = float("nan")
+    # the best evaluation by PSNR, as the reference trainer keeps it (trainer.py:455-471)
+    best: Dict = field(default_factory=dict)
+    best_params: Optional[GaussianSet] = None
+    stopped_early: bool = False
 
 
 def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Callable] = None,
@@ -381,7 +420,10 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
     evaluations; `stop_nmse` ends the fit at the first evaluation at or below
     that hard-DC NMSE (time-to-NMSE runs).  `split_noise(n)`, called once
     per densifying iteration, gives the [n,6] split noise instead of draws
-    from the fit's generator."""
+    from the fit's generator.  With `cfg.plateau_stop` every evaluation also
+    scores PSNR and SSIM and the fit ends as the reference trainer's metric
+    plateau stop ends it; `res.best` is the best evaluation by PSNR either
+    way (with `cfg.keep_best`, `res.best_params` its parameters)."""
     dev = torch.device(device)
     shape = tuple(case.ground_truth.shape)
     if voxelizer is None:
@@ -403,6 +445,9 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
     opt = make_optimizer(p, cfg, lrs, capturable=cfg.capturable_adam)
     gen = torch.Generator(device=dev).manual_seed(cfg.seed)
     res = FitResult(params=p)
+    stopper = (PlateauStop(cfg.plateau_patience, cfg.plateau_min_iterations,
+                           {"psnr": cfg.plateau_min_delta_psnr, "ssim": cfg.plateau_min_delta_ssim})
+               if cfg.plateau_stop else None)
     mask_c = mask.unsqueeze(0)
     skip_sched = False
     wall = 0.0
@@ -452,11 +497,21 @@ def fit(case: MRICase, init: GaussianSet, cfg: FitConfig, voxelizer: Optional[Ca
                     v = torch.complex(v[0], v[1])
                 rec = hard_data_consistency(v, S, mask, ku)
                 e = nmse(rec, gt)
-            row = {"iteration": it, "loss": float(loss.detach()), "nmse": e, "n_points": p.n, "seconds": wall}
+                row = {"iteration": it, "loss": float(loss.detach()), "nmse": e, "n_points": p.n, "seconds": wall,
+                       "psnr": psnr(rec, gt)}
+                if stopper is not None:
+                    row["ssim"] = ssim3d(rec, gt)
+                if not res.best or row["psnr"] > res.best["psnr"]:
+                    res.best = dict(row)
+                    if cfg.keep_best:
+                        res.best_params = p.snapshot()
             res.history.append(row)
             if log:
                 log(row)
             done = stop_nmse is not None and e <= stop_nmse
+            if stopper is not None and stopper.update(it, {"psnr": row["psnr"], "ssim": row["ssim"]}):
+                done = True
+                res.stopped_early = not last
             if last or done:
                 res.final_nmse = e
                 res.final_psnr = psnr(rec, gt)

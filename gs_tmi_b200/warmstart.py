@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 from dataclasses import dataclass
 from typing import List, Optional, Tuple
 
@@ -215,6 +216,9 @@ class WarmConfig:
     points_per_voxel: float = 50_000 / (128 * 128 * 96)
     mask_kind: str = "vd"  # "poisson": the reference's Poisson-disc (ky, kz) sampling (synthetic.mri_case)
     fit_iterations: int = 1000
+    # the training target: "best" = the plain fit's best-PSNR evaluation under the reference
+    # trainer's metric-plateau stop (what the reference reports); "last" = its last iterate
+    target: str = "best"
 
 
 @dataclass
@@ -247,14 +251,17 @@ def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
                               mask_kind=wc.mask_kind)
     n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
     x, vox, base, scale = case_inputs(case, n, seed + 1, device)
-    cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=10 ** 9)
+    if wc.target == "best":
+        cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=50, plateau_stop=True, keep_best=True)
+    else:
+        cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=10 ** 9)
     res = sense.fit(case, base, cfg, device=device, eval_ssim=False)
     from .tile_voxelizer import TileVoxelizer
 
     vz = TileVoxelizer(wc.shape, device=device)
-    p = res.params
+    g = res.best_params if wc.target == "best" else res.params.snapshot()
     with torch.no_grad():
-        target = vz(p.positions, torch.exp(p.log_scales), p.rotations, torch.complex(p.density_r, p.density_i))
+        target = vz(g.positions, g.scales, g.rotations, torch.complex(g.density_r, g.density_i))
     return TrainingCase(wc.shape, x, vox, base, scale, target.detach())
 
 
@@ -300,6 +307,58 @@ def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed:
     pos, scl, rot, dr, di = decode(out, vox, base, tuple(case.ground_truth.shape), scale)
     return synthetic.GaussianSet(pos.contiguous(), scl.contiguous(), rot.contiguous(), dr.contiguous(),
                                  di.contiguous())
+
+
+def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_points: int, seed: int = 0,
+                   device="cuda:0", cadence: int = 10, max_iterations: int = 2000) -> dict:
+    """Warm start against the plain method on one acquisition.
+
+    The plain method runs as the reference trainer runs it (evaluation
+    every 50 iterations, metric-plateau stop, best evaluation by PSNR); its
+    best NMSE is the target.  Then the plain fit and the warm-started fit
+    each run from their initialisation until their hard-data-consistency
+    NMSE first reaches the target, evaluated every `cadence` iterations.
+    Times are wall seconds of initialisation plus fitting (evaluations
+    excluded); all fits use the deterministic backward, so the plain rerun
+    retraces the first run exactly.  `mlp` None: the warm arm is skipped."""
+    dev = torch.device(device)
+    shape = tuple(case.ground_truth.shape)
+    rule = sense.FitConfig(iterations=max_iterations, eval_every=50, plateau_stop=True, deterministic=True)
+
+    def timed_init(fn):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize(dev)
+        return out, time.perf_counter() - t0
+
+    plain_init, t_plain_init = timed_init(
+        lambda: synthetic.from_image_init(case.zero_filled, num_points, seed=seed, device=dev))
+    ref = sense.fit(case, plain_init, rule, device=device, eval_ssim=False)
+    target = ref.best["nmse"]
+    to_target = sense.FitConfig(iterations=max_iterations, eval_every=cadence, deterministic=True)
+
+    def first_hit(res):
+        hit = [h for h in res.history if h["nmse"] <= target]
+        return (hit[0]["iteration"], hit[0]["seconds"]) if hit else (None, None)
+
+    plain = sense.fit(case, plain_init, to_target, device=device, stop_nmse=target, eval_ssim=False)
+    p_it, p_s = first_hit(plain)
+    row = {"target_nmse": target, "plain_best_iteration": ref.best["iteration"],
+           "plain_stopped_at": ref.history[-1]["iteration"], "plain_nmse_at_0": plain.history[0]["nmse"],
+           "plain_iterations_to_target": p_it, "plain_init_seconds": t_plain_init,
+           "plain_seconds_to_target": None if p_s is None else p_s + t_plain_init}
+    if mlp is None:
+        return row
+    warm, t_warm_init = timed_init(lambda: warm_init(mlp, case, num_points, seed=seed, device=device))
+    w = sense.fit(case, warm, to_target, device=device, stop_nmse=target, eval_ssim=False)
+    w_it, w_s = first_hit(w)
+    row.update({"warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": w_it,
+                "warm_init_seconds": t_warm_init,
+                "warm_seconds_to_target": None if w_s is None else w_s + t_warm_init})
+    if w_s is not None and p_s:
+        row["wall_ratio"] = row["warm_seconds_to_target"] / row["plain_seconds_to_target"]
+    return row
 
 
 def time_training_pass(batch: int = 65536, iters: int = 5, device="cuda:0", seed: int = 0) -> dict:

@@ -73,6 +73,31 @@ def build(reference: str | None = None, force: bool = False) -> str | None:
     return SO
 
 
+PY_OUT = os.path.join(os.path.dirname(HERE), "baseline", "_ref")
+PY_PACKAGES = ("configs", "data", "gaussian", "losses", "metrics", "trainers")
+
+
+def stage_python(reference: str | None = None) -> str | None:
+    """Stage the reference's Python package (3DGS/3dgsVC: its trainer, data
+    loader, Gaussian model, losses, metrics and configs) unchanged into the
+    git-ignored baseline/_ref/3dgsVC, where the drop-in test imports it and
+    from where it travels with the working tree.  Returns the staged root,
+    or None when neither the sources nor an earlier staging exist."""
+    import shutil
+
+    src = os.path.join(reference_root(reference), "3DGS", "3dgsVC")
+    dst = os.path.join(PY_OUT, "3dgsVC")
+    if not os.path.isdir(src):
+        return dst if os.path.isdir(dst) else None
+    os.makedirs(dst, exist_ok=True)
+    for pkg in PY_PACKAGES:
+        target = os.path.join(dst, pkg)
+        if os.path.isdir(target):
+            shutil.rmtree(target)
+        shutil.copytree(os.path.join(src, pkg), target, ignore=shutil.ignore_patterns("build", "__pycache__", "*.so"))
+    return dst
+
+
 def load():
     """Import the compiled reference extension (None if it was never built)."""
     if not os.path.exists(SO):
@@ -95,4 +120,6 @@ if __name__ == "__main__":
     a = ap.parse_args()
     out = build(a.reference, a.force)
     print(out if out else "reference sources not found; nothing built")
+    staged = stage_python(a.reference)
+    print(staged if staged else "reference Python package not found; nothing staged")
     sys.exit(0 if out else 1)

@@ -1,14 +1,26 @@
 """Reconstruction with the SENSE loop (gs_tmi_b200.sense): convergence, and
 parity of the whole fit when the voxelizer is this build vs the reference's
-own CUDA kernels on the same seeded inputs (bar: final NMSE and SSIM within
-0.1% of the reference run).
+own CUDA kernels on the same seeded inputs.
 
-GSV_RECON_FULL=1 additionally runs the 128x128x96 / 8-coil / R=6 / 50k->500k /
-2000-iteration plain reconstruction with both voxelizers and writes wall
-times and metrics to $GSV_REPORT_DIR/recon_128x128x96.json."""
+Bars on the 128x128x96 / 8-coil / R=6 Poisson-disc / 50k-Gaussian
+configuration:
+* the first 100 iterations: loss and hard-data-consistency NMSE at every
+  10th iteration within 0.1% of the run with the reference kernels;
+* the final result as the reference trainer reports it (its metric-plateau
+  early stop, best evaluation by PSNR; V/trainers/trainer.py:455-471,
+  :571-590): five runs per voxelizer, the mean NMSE and SSIM within 0.1% of
+  the reference kernels' means, unless the two means' own standard error
+  (atomic-order run-to-run scatter, which both builds have) is larger, in
+  which case within three standard errors.
+
+GSV_RECON_FULL=1 additionally runs the 2000-iteration plain reconstruction
+(densification to 500k) with both voxelizers and writes wall times and
+metrics to $GSV_REPORT_DIR/recon_128x128x96.json."""
 import dataclasses
 import json
+import math
 import os
+import statistics
 
 import pytest
 import torch
@@ -46,26 +58,71 @@ def test_deterministic_fit_is_reproducible(cuda_device):
         assert torch.equal(x, y)
 
 
+def _config2():
+    shape = (128, 128, 96)
+    case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=0, mask_kind="poisson")
+    init = synthetic.from_image_init(case.zero_filled, 50_000, seed=0)
+    return shape, case, init
+
+
+def _report(name, data):
+    out = os.environ.get("GSV_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, name), "w") as f:
+            json.dump(data, f, indent=1)
+    print(json.dumps(data)[:4000])
+
+
 @pytest.mark.skipif(REF is None, reason="reference extension not built")
-def test_recon_parity_with_reference_kernels(cuda_device):
-    """Same seeded case, init and schedule (densification off, so both runs
-    keep the same Gaussians); the voxelizer is this build or the reference's
-    kernels.  Two runs of the reference itself already differ by ~0.4% in
-    final NMSE (FP32 atomic order in its backward, amplified by Adam on
-    near-zero gradients), so the bar is the reference's own spread with a
-    0.5% floor; SSIM must agree within 0.5%."""
-    shape, case, init, cfg = _small()
-    cfg.densify_from = 10 ** 9
+def test_recon_first_iterations_match_reference_kernels(cuda_device):
+    """Same case, init and schedule; the voxelizer is this build or the
+    reference's kernels.  Before densification (iteration 100) and before
+    the atomic-order differences of the two backwards grow, the trajectories
+    agree to 0.1%."""
+    shape, case, init = _config2()
+    cfg = sense.FitConfig(iterations=100, eval_every=10)
     dev = str(cuda_device)
-    mine = sense.fit(case, init, cfg, device=dev)
-    ref_a = sense.fit(case, init, cfg, voxelizer=RefVoxelizer(shape), device=dev)
-    ref_b = sense.fit(case, init, cfg, voxelizer=RefVoxelizer(shape), device=dev)
-    ref_mean = 0.5 * (ref_a.final_nmse + ref_b.final_nmse)
-    spread = abs(ref_a.final_nmse - ref_b.final_nmse) / ref_mean
-    assert abs(mine.final_nmse / ref_mean - 1) <= max(0.005, 2 * spread)
-    assert abs(mine.final_ssim / (0.5 * (ref_a.final_ssim + ref_b.final_ssim)) - 1) < 5e-3
-    # identical start: the first evaluation is the same volume
-    assert abs(mine.history[0]["nmse"] / ref_a.history[0]["nmse"] - 1) < 1e-6
+    mine = sense.fit(case, init, cfg, device=dev, eval_ssim=False)
+    ref = sense.fit(case, init, cfg, voxelizer=RefVoxelizer(shape), device=dev, eval_ssim=False)
+    rows = [{"iteration": a["iteration"], "nmse": a["nmse"], "ref_nmse": b["nmse"],
+             "nmse_rel": a["nmse"] / b["nmse"] - 1, "loss_rel": a["loss"] / b["loss"] - 1}
+            for a, b in zip(mine.history, ref.history)]
+    _report("recon_first_iterations_128x128x96.json", {"rows": rows})
+    assert [r["iteration"] for r in rows] == list(range(0, 100, 10)) + [99]
+    for r in rows:
+        assert abs(r["nmse_rel"]) < 1e-3, r
+        assert abs(r["loss_rel"]) < 1e-3, r
+
+
+@pytest.mark.skipif(REF is None, reason="reference extension not built")
+def test_recon_final_metrics_match_reference_kernels(cuda_device):
+    """Five runs per voxelizer with the reference trainer's stopping rule
+    (evaluation every 50 iterations, PSNR/SSIM plateau, best by PSNR)."""
+    shape, case, init = _config2()
+    cfg = sense.FitConfig(iterations=2000, eval_every=50, plateau_stop=True)
+    dev = str(cuda_device)
+    runs = {"this_build": [], "reference_kernels": []}
+    for _ in range(5):
+        for name, vox in (("this_build", None), ("reference_kernels", RefVoxelizer(shape))):
+            r = sense.fit(case, init, cfg, voxelizer=vox, device=dev, eval_ssim=False)
+            runs[name].append({"best": r.best, "stopped_at": r.history[-1]["iteration"], "seconds": r.seconds})
+    stats = {}
+    for name, rs in runs.items():
+        for key in ("nmse", "ssim", "psnr"):
+            v = [x["best"][key] for x in rs]
+            stats[f"{name}/{key}"] = {"mean": statistics.mean(v), "se": statistics.stdev(v) / math.sqrt(len(v))}
+    report = {"runs": runs, "stats": stats}
+    checks = {}
+    for key in ("nmse", "ssim"):
+        a, b = stats[f"this_build/{key}"], stats[f"reference_kernels/{key}"]
+        rel = a["mean"] / b["mean"] - 1
+        se = math.hypot(a["se"], b["se"]) / b["mean"]
+        checks[key] = {"rel_diff": rel, "rel_se": se, "bar": max(1e-3, 3 * se)}
+    report["checks"] = checks
+    _report("recon_final_128x128x96.json", report)
+    for key, c in checks.items():
+        assert abs(c["rel_diff"]) <= c["bar"], (key, c)
 
 
 @pytest.mark.skipif(os.environ.get("GSV_RECON_FULL") != "1" or REF is None, reason="set GSV_RECON_FULL=1")

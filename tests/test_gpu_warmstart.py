@@ -119,54 +119,60 @@ def test_warm_start_gains_over_intensity_seeding(cuda_device):
     assert w.history[-1]["nmse"] < p.history[-1]["nmse"]
 
 
-@pytest.mark.skipif(os.environ.get("GSV_WARM_FULL") != "1", reason="set GSV_WARM_FULL=1")
-def test_full_time_to_nmse(cuda_device):
-    dev = str(cuda_device)
-    mask_kind = os.environ.get("GSV_WARM_MASK", "vd")  # "poisson": the reference's Poisson-disc sampling
+def _time_to_target_eval(dev, n_train, n_eval, steps, mask_kind="poisson", report_name=None):
+    """Train on `n_train` plain fits of 96^3 phantoms (the reference's
+    stopping rule picks each fit's best iterate as the target), then time
+    warm start and plain method to the plain method's final NMSE on
+    `n_eval` held-out 128x128x96, 8-coil, R=6 acquisitions."""
     wc = warmstart.WarmConfig(mask_kind=mask_kind)
-    n_train = int(os.environ.get("GSV_WARM_TRAIN_PHANTOMS", "48"))
-    n_eval = int(os.environ.get("GSV_WARM_EVAL_PHANTOMS", "4"))
     t0 = time.perf_counter()
     cases = [warmstart.training_case(1000 + 17 * s, wc, device=dev) for s in range(n_train)]
     t_data = time.perf_counter() - t0
     mlp = warmstart.WarmStartMLP(dev, seed=0)
     t0 = time.perf_counter()
-    losses = warmstart.train(mlp, cases, steps=int(os.environ.get("GSV_WARM_STEPS", "2000")))
+    losses = warmstart.train(mlp, cases, steps=steps)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     shape = (128, 128, 96)
-    cfg = sense.FitConfig(iterations=2000, eval_every=25, max_points=500_000)
     rows = []
     for e in range(n_eval):
         case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e, mask_kind=mask_kind)
-        plain = sense.fit(case, synthetic.from_image_init(case.zero_filled, 50_000, seed=e), cfg, device=dev,
-                          eval_ssim=True)
-        target = plain.final_nmse
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        warm = warmstart.warm_init(mlp, case, 50_000, seed=e, device=dev)
-        torch.cuda.synchronize()
-        t_init = time.perf_counter() - t0
-        w = sense.fit(case, warm, cfg, device=dev, stop_nmse=target, eval_ssim=True)
-        reached = [h for h in w.history if h["nmse"] <= target]
-        it = reached[0]["iteration"] if reached else None
-        secs = (reached[0]["seconds"] + t_init) if reached else None
-        rows.append({"phantom": e, "plain_final_nmse": target, "plain_final_ssim": plain.final_ssim,
-                     "plain_seconds": plain.seconds, "plain_nmse_at_0": plain.history[0]["nmse"],
-                     "warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": it,
-                     "warm_seconds_to_target": secs, "warm_init_seconds": t_init,
-                     "wall_ratio": (secs / plain.seconds) if secs else None})
-    report = {"mask": mask_kind, "train_phantoms": n_train, "train_examples": int(sum(c.features.shape[0] for c in cases)),
-              "data_seconds": t_data, "train_seconds": t_train, "final_train_loss": losses[-1],
-              "eval": rows}
-    ratios = [r["wall_ratio"] for r in rows if r["wall_ratio"] is not None]
-    report["median_wall_ratio"] = sorted(ratios)[len(ratios) // 2] if ratios else None
+        rows.append(dict(warmstart.time_to_target(mlp, case, 50_000, seed=e, device=dev), phantom=e))
+    ratios = sorted(r["wall_ratio"] for r in rows if r.get("wall_ratio") is not None)
+    report = {"mask": mask_kind, "train_phantoms": n_train, "eval_phantoms": n_eval, "train_steps": steps,
+              "train_examples": int(sum(c.features.shape[0] for c in cases)), "data_seconds": t_data,
+              "train_seconds": t_train, "first_train_loss": losses[0], "final_train_loss": losses[-1],
+              "median_wall_ratio": ratios[len(ratios) // 2] if ratios else None,
+              "reached": sum(r.get("warm_iterations_to_target") is not None for r in rows),
+              "warm_starts_lower": sum(r["warm_nmse_at_0"] < r["plain_nmse_at_0"] for r in rows), "eval": rows}
     out = os.environ.get("GSV_REPORT_DIR")
-    if out:
+    if out and report_name:
         os.makedirs(out, exist_ok=True)
-        with open(os.path.join(out, "warmstart_eval.json"), "w") as f:
+        with open(os.path.join(out, report_name), "w") as f:
             json.dump(report, f, indent=1)
     print(json.dumps({k: v for k, v in report.items() if k != "eval"}), json.dumps(rows))
-    # the plain method's final NMSE is reached, in at most half its wall time
-    assert all(r["warm_iterations_to_target"] is not None for r in rows)
-    assert report["median_wall_ratio"] <= 0.5
+    return report
+
+
+def test_time_to_target_small(cuda_device):
+    """Reduced config-5 evaluation that every GPU test run performs: 12
+    training phantoms, 2 held-out acquisitions on the reference's
+    Poisson-disc sampling.  The warm start must reach the plain method's
+    final NMSE on both."""
+    rep = _time_to_target_eval(str(cuda_device), n_train=12, n_eval=2, steps=600,
+                               report_name="warmstart_time_to_target_small.json")
+    assert rep["reached"] == rep["eval_phantoms"]
+
+
+@pytest.mark.skipif(os.environ.get("GSV_WARM_FULL") != "1", reason="set GSV_WARM_FULL=1")
+def test_full_time_to_nmse(cuda_device):
+    """Config 5: GSV_WARM_TRAIN_PHANTOMS (default 2000) training phantoms,
+    GSV_WARM_EVAL_PHANTOMS (default 50) held-out acquisitions; the median
+    warm/plain wall ratio to the plain method's final NMSE must be <= 0.5."""
+    rep = _time_to_target_eval(str(cuda_device), n_train=int(os.environ.get("GSV_WARM_TRAIN_PHANTOMS", "2000")),
+                               n_eval=int(os.environ.get("GSV_WARM_EVAL_PHANTOMS", "50")),
+                               steps=int(os.environ.get("GSV_WARM_STEPS", "6000")),
+                               mask_kind=os.environ.get("GSV_WARM_MASK", "poisson"),
+                               report_name="warmstart_eval.json")
+    assert rep["reached"] == rep["eval_phantoms"]
+    assert rep["median_wall_ratio"] <= 0.5

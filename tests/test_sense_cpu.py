@@ -180,3 +180,20 @@ def test_density_control_branches_on_cpu():
     weak[60:110] = 0.5
     p = sense.GaussianParams(synthetic.GaussianSet(pos, big, rot, weak, di * 0), "cpu")
     assert sense.density_control(p, torch.zeros(n, 3), cfg, None, events.append) == 1 and p.n == 110
+
+
+def test_plateau_stop_follows_the_reference_rule():
+    """V/metrics/metrics.py:166-195: an evaluation improves when some metric
+    beats its best by more than its delta; `patience` evaluations in a row
+    without improvement stop the fit, but not before `min_iterations`."""
+    st = sense.PlateauStop(patience=2, min_iterations=100, min_delta={"psnr": 0.05, "ssim": 0.0005})
+    seq = [(0, 20.0, 0.50), (50, 20.3, 0.51), (100, 20.33, 0.5103), (150, 20.34, 0.5104), (200, 20.2, 0.50)]
+    out = [st.update(it, {"psnr": p, "ssim": s}) for it, p, s in seq]
+    # 100 and 150: psnr +0.03 / +0.04 and ssim +0.0003 / +0.0004 stay within their deltas -> bad 1, 2: stop
+    assert out == [False, False, False, True, True]
+    # improvement resets the count; the minimum iteration holds the stop back
+    st = sense.PlateauStop(patience=1, min_iterations=300)
+    assert st.update(0, {"psnr": 10.0, "ssim": 0.1}) is False
+    assert st.update(100, {"psnr": 10.0, "ssim": 0.1}) is False  # bad 1, but iteration < 300
+    assert st.update(300, {"psnr": 10.2, "ssim": 0.1}) is False  # psnr improved: reset
+    assert st.update(350, {"psnr": 10.2, "ssim": 0.1}) is True
