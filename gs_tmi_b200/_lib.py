@@ -21,6 +21,7 @@ GSV_ERR_TOO_MANY_PAIRS = 5
 GSV_FLAG_CAPACITY_OVERFLOW = 0x1
 GSV_FLAG_EMPTY_BOX = 0x2
 GSV_FLAG_TOO_MANY_PAIRS = 0x4
+GSV_FLAG_SCAN_STALLED = 0x8
 
 GSV_BACKWARD_DETERMINISTIC = 0x1
 GSV_TUNE_NO_CULL = 0x1

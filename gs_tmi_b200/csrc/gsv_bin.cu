@@ -52,6 +52,16 @@ int sort_end_bit(int64_t ntiles) {
     return bits;
 }
 
+// The preprocess scans the per-Gaussian pair counts in one pass (decoupled
+// look-back): blocks of kPrepThreads Gaussians, one 64-bit look-back word per
+// block after the Status struct, all cleared by the one memset of the status
+// region that starts every preprocess.
+constexpr int kPrepThreads = 256;
+__host__ __device__ inline int64_t prep_blocks(int64_t n) { return (n + 1 + kPrepThreads - 1) / kPrepThreads; }
+__host__ __device__ inline size_t status_bytes(int64_t n) {
+    return sizeof(Status) + size_t(prep_blocks(n)) * sizeof(unsigned long long);
+}
+
 GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
     GaussLayout L{};
     size_t scan_bytes = 0;
@@ -67,7 +77,7 @@ GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
     L.scan_tmp = o; o = align_up(o + scan_bytes);
     L.ranges = o;   o = align_up(o + size_t(si.ntiles) * sizeof(int2));
     L.accum = o;    o = align_up(o + size_t(n) * kMomStride * sizeof(float));
-    L.status = o;   o = align_up(o + sizeof(Status));
+    L.status = o;   o = align_up(o + status_bytes(n));
     L.total = o;
     return L;
 }
@@ -154,58 +164,130 @@ __device__ __forceinline__ int64_t tile_box(const DevShape& s, const float c[3],
     return cnt;
 }
 
-__global__ void __launch_bounds__(256) k_prepare(const float* __restrict__ pos,
-                                                 const float* __restrict__ scl,
-                                                 const float* __restrict__ rot,
-                                                 const float* __restrict__ dr,
-                                                 const float* __restrict__ di, int64_t n,
-                                                 const int32_t* __restrict__ live, DevShape s,
-                                                 Rec* __restrict__ recs, float4* __restrict__ ext,
-                                                 int4* __restrict__ boxes,
-                                                 int64_t* __restrict__ counts, Status* status) {
-    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g == 0) counts[n] = 0;
-    if (g >= n) return;
-    if (live && g >= int64_t(*live)) {  // parked row: no tiles, no contribution
+// Look-back word of a block: flag in the top two bits, an int64 pair count
+// below.  kLbAgg: the block's own total; kLbPre: the total of every block up
+// to and including it.
+constexpr unsigned long long kLbAgg = 1ull << 62, kLbPre = 2ull << 62, kLbVal = (1ull << 62) - 1;
+constexpr int kLbSpinLimit = 1 << 22;  // polls of one predecessor's word before giving up
+
+__device__ __forceinline__ unsigned long long lb_load(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Preprocess (center, radius, quadratic-form coefficients, tight extent, tile
+// box) of one Gaussian per thread, and the exclusive scan of the Gaussians'
+// pair counts into `offsets` (offsets[n] = pair total) in the same launch.
+// Blocks take their position in the scan from a counter in the status
+// region, so every block a block waits for has already started; it waits
+// only for its predecessors' published totals, each wait bounded (on
+// time-out GSV_FLAG_SCAN_STALLED is latched and the block publishes anyway,
+// so no later block waits the full limit again).
+__global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restrict__ pos,
+                                                          const float* __restrict__ scl,
+                                                          const float* __restrict__ rot,
+                                                          const float* __restrict__ dr,
+                                                          const float* __restrict__ di, int64_t n,
+                                                          const int32_t* __restrict__ live, DevShape s,
+                                                          Rec* __restrict__ recs, float4* __restrict__ ext,
+                                                          int4* __restrict__ boxes,
+                                                          int64_t* __restrict__ offsets, Status* status) {
+    __shared__ int bid_s;
+    __shared__ int64_t warp_tot[kPrepThreads / 32];
+    __shared__ int64_t block_base;
+    if (threadIdx.x == 0) bid_s = atomicAdd(&status->pad[1], 1);
+    __syncthreads();
+    const int64_t bid = bid_s;
+    const int64_t g = bid * kPrepThreads + threadIdx.x;
+    int64_t cnt = 0;
+    if (g < n && live && g >= int64_t(*live)) {  // parked row: no tiles, no contribution
         recs[g] = Rec{};
         ext[g] = make_float4(0.f, 0.f, 0.f, 0.f);
         boxes[g] = make_int4(0, 0, 0, 0);
-        counts[g] = 0;
-        return;
-    }
-    float p[3], sc[3], q[4];
+    } else if (g < n) {
+        float p[3], sc[3], q[4];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        p[a] = pos[g * 3 + a];
-        sc[a] = scl[g * 3 + a];
-    }
+        for (int a = 0; a < 3; ++a) {
+            p[a] = pos[g * 3 + a];
+            sc[a] = scl[g * 3 + a];
+        }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) q[k] = rot[g * 4 + k];
-    float c[3], sv[3];
+        for (int k = 0; k < 4; ++k) q[k] = rot[g * 4 + k];
+        float c[3], sv[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        // center_vox = (positions + 1.0) * 0.5 * shape - 0.5   (:284)
-        c[a] = __fsub_rn(__fmul_rn(__fmul_rn(__fadd_rn(p[a], 1.0f), 0.5f), s.shape_f[a]), 0.5f);
-        sv[a] = __fmul_rn(sc[a], s.hs[a]);  // scale_vox (:285)
+        for (int a = 0; a < 3; ++a) {
+            // center_vox = (positions + 1.0) * 0.5 * shape - 0.5   (:284)
+            c[a] = __fsub_rn(__fmul_rn(__fmul_rn(__fadd_rn(p[a], 1.0f), 0.5f), s.shape_f[a]), 0.5f);
+            sv[a] = __fmul_rn(sc[a], s.hs[a]);  // scale_vox (:285)
+        }
+        const float r = __fmul_rn(nanmax3(sv[0], sv[1], sv[2]), 3.0f);  // radius_vox (:286)
+        float qc[6];
+        qcoef_from_params(sc, q, s.ih, qc);
+        Rec R;
+        R.c0 = c[0]; R.c1 = c[1]; R.c2 = c[2];
+        R.q00 = qc[0]; R.q01x2 = qc[1]; R.q02x2 = qc[2]; R.q11 = qc[3]; R.q12x2 = qc[4]; R.q22 = qc[5];
+        R.rho_r = dr[g]; R.rho_i = di[g]; R.pad = 0.0f;
+        recs[g] = R;
+        ext[g] = tight_extent(qc);
+        int4 box;
+        cnt = tile_box(s, c, r, &box);
+        if (cnt <= 0) {
+            atomicOr(&status->flags, GSV_FLAG_EMPTY_BOX);
+            cnt = 0;
+            box.w = 0;
+        }
+        boxes[g] = box;
     }
-    const float r = __fmul_rn(nanmax3(sv[0], sv[1], sv[2]), 3.0f);  // radius_vox (:286)
-    float qc[6];
-    qcoef_from_params(sc, q, s.ih, qc);
-    Rec R;
-    R.c0 = c[0]; R.c1 = c[1]; R.c2 = c[2];
-    R.q00 = qc[0]; R.q01x2 = qc[1]; R.q02x2 = qc[2]; R.q11 = qc[3]; R.q12x2 = qc[4]; R.q22 = qc[5];
-    R.rho_r = dr[g]; R.rho_i = di[g]; R.pad = 0.0f;
-    recs[g] = R;
-    ext[g] = tight_extent(qc);
-    int4 box;
-    int64_t cnt = tile_box(s, c, r, &box);
-    if (cnt <= 0) {
-        atomicOr(&status->flags, GSV_FLAG_EMPTY_BOX);
-        cnt = 0;
-        box.w = 0;
+    // block-wide inclusive scan of the counts
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
     }
-    boxes[g] = box;
-    counts[g] = cnt;
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    int64_t warp_base = 0, block_tot = 0;
+#pragma unroll
+    for (int w = 0; w < kPrepThreads / 32; ++w) {
+        if (w < warp) warp_base += warp_tot[w];
+        block_tot += warp_tot[w];
+    }
+    if (threadIdx.x == 0) {
+        unsigned long long* lb = reinterpret_cast<unsigned long long*>(status + 1);
+        int64_t base = 0;
+        if (bid == 0) {
+            lb_store(&lb[0], kLbPre | (unsigned long long)block_tot);
+        } else {
+            lb_store(&lb[bid], kLbAgg | (unsigned long long)block_tot);
+            int64_t j = bid - 1;
+            int spins = 0;
+            while (true) {
+                const unsigned long long v = lb_load(&lb[j]);
+                const unsigned long long f = v & ~kLbVal;
+                if (f == 0) {
+                    if (++spins > kLbSpinLimit) {
+                        atomicOr(&status->flags, GSV_FLAG_SCAN_STALLED);
+                        break;
+                    }
+                    continue;
+                }
+                spins = 0;
+                base += int64_t(v & kLbVal);
+                if (f == kLbPre || j == 0) break;
+                --j;
+            }
+            lb_store(&lb[bid], kLbPre | (unsigned long long)(base + block_tot));
+        }
+        block_base = base;
+    }
+    __syncthreads();
+    if (g <= n) offsets[g] = block_base + warp_base + incl - cnt;
 }
 
 __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ center,
@@ -412,17 +494,13 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
     if (ws_gauss_bytes < L.total) return GSV_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Status* status = at<Status>(ws_gauss, L.status);
-    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(Status), st));
-    k_prepare<<<grid_for(n + 1, 256), 256, 0, st>>>(p->positions, p->scales, p->rotations, p->density_r,
-                                                    p->density_i, n, live, dev_shape(si), at<Rec>(ws_gauss, L.rec),
-                                                    at<float4>(ws_gauss, L.ext),
-                                                    at<int4>(ws_gauss, L.box), at<int64_t>(ws_gauss, L.counts),
-                                                    status);
+    // status flags, the block counter and the scan's look-back words
+    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, status_bytes(n), st));
+    k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, 0, st>>>(
+        p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
+        at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),
+        at<int64_t>(ws_gauss, L.offsets), status);
     GSV_LAUNCH_CHECK();
-    size_t scan_bytes = L.scan_tmp_bytes;
-    GSV_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at<void>(ws_gauss, L.scan_tmp), scan_bytes,
-                                               at<int64_t>(ws_gauss, L.counts),
-                                               at<int64_t>(ws_gauss, L.offsets), int(n + 1), st));
     if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
     return GSV_OK;
 }

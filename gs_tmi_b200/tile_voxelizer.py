@@ -99,6 +99,8 @@ class BinPlan:
 
 
 def _raise_flags(flags: int, total: int):
+    if flags & _lib.GSV_FLAG_SCAN_STALLED:
+        raise RuntimeError("the preprocess's pair-count scan timed out waiting for a block (results invalid)")
     if flags & _lib.GSV_FLAG_EMPTY_BOX:
         raise ValueError("a Gaussian has an empty tile box (negative scale radius)")
     if flags & _lib.GSV_FLAG_TOO_MANY_PAIRS or total > INT32_MAX:

@@ -65,6 +65,7 @@ typedef enum gsv_status {
 #define GSV_FLAG_CAPACITY_OVERFLOW 0x1
 #define GSV_FLAG_EMPTY_BOX 0x2
 #define GSV_FLAG_TOO_MANY_PAIRS 0x4
+#define GSV_FLAG_SCAN_STALLED 0x8 /* a bounded wait of the preprocess's pair-count scan ran out */
 
 /* Backward options. */
 #define GSV_BACKWARD_DETERMINISTIC 0x1 /* fixed-order reduction: bitwise reproducible gradients */

@@ -146,3 +146,18 @@ def test_density_host_queries():
     assert density.initial_rows(1000, 500_000) == 65_536
     assert density.initial_rows(400_000, 500_000) == 500_000
     assert density.initial_rows(600_000, 500_000) == 600_000
+
+
+def test_flag_and_status_constants_mirror_the_header():
+    """Every GSV_FLAG_*, GSV_BACKWARD_* and GSV_TUNE_* #define of
+    include/gsv.h has the same value in the ctypes binding."""
+    import re
+
+    from gs_tmi_b200 import _lib
+
+    text = open(os.path.join(ROOT, "include", "gsv.h")).read()
+    defs = dict(re.findall(r"^#define\s+(GSV_(?:FLAG|BACKWARD|TUNE|DENSITY)_\w+)\s+(0x[0-9a-fA-F]+|\d+)", text,
+                           flags=re.M))
+    assert "GSV_FLAG_SCAN_STALLED" in defs
+    for name, value in defs.items():
+        assert getattr(_lib, name) == int(value, 0), name
