@@ -461,7 +461,6 @@ class Workload:
         vol = self.vol = torch.empty(shape, dtype=torch.complex64, device=dev)
         gp = GsvParams(*(t.data_ptr() for t in params), n)
         gg = GsvGrads(*(o.data_ptr() for o in outs))
-        st = _stream(dev)
         wsg, wsp = _ptr(plan.ws_gauss), _ptr(plan.ws_pairs)
         self.tuning, self.tune_times, self.tile_pick, self.tile_times = None, {}, None, {}
         if not args.no_autotune:
@@ -474,16 +473,18 @@ class Workload:
             self.tile_pick, _, self.tile_times = tuner.pick_tile_size(params, shape, flags)
         tref = ctypes.byref(self.tuning) if self.tuning is not None else None
 
+        # every launch goes to the stream current at call time (a graph capture's stream included)
         def prep_bin():
+            st = _stream(dev)
             check(lib.gsv_prepare(ctypes.byref(gp), gshape, wsg, plan.gauss_bytes, None, st), "prepare")
             check(lib.gsv_bin(gshape, n, wsg, wsp, plan.pair_bytes, cap, st), "bin")
 
         def fwd():
-            check(lib.gsv_forward_ex(gshape, n, wsg, wsp, cap, _ptr(vol), tref, st), "forward")
+            check(lib.gsv_forward_ex(gshape, n, wsg, wsp, cap, _ptr(vol), tref, _stream(dev)), "forward")
 
         def bwd():
             check(lib.gsv_backward_ex(ctypes.byref(gp), gshape, wsg, wsp, cap, _ptr(gvd), ctypes.byref(gg), flags,
-                                      tref, st), "backward")
+                                      tref, _stream(dev)), "backward")
 
         self.prep_bin, self.fwd, self.bwd = prep_bin, fwd, bwd
         # E from the executed binning, and what the render kernels execute of it
@@ -511,8 +512,12 @@ class Workload:
         torch.cuda.current_stream(dev).wait_stream(side)
         torch.cuda.synchronize(dev)
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=side):
-            self.step()
+        import warnings
+
+        with warnings.catch_warnings():
+            warnings.filterwarnings("error", message=".*Graph is empty.*")  # an empty capture: fail
+            with torch.cuda.graph(g, stream=side):
+                self.step()
         torch.cuda.synchronize(dev)
         return g
 
@@ -605,7 +610,6 @@ def roofline_of(wl, t, peak_ops, pk, pk_kind, sm_mhz):
             "forward": {"achieved": ach_fwd / 1e12, "frac": ach_fwd / peak_ops, "ops_per_eval": OPS_FWD},
             "work": {"candidates": wl.evals, "included": useful, "evaluated_after_cull": c["evaluated"],
                      "exp_block_lanes": c["exp_block_lanes"], "empty_kept_slots": c["empty_kept_slots"],
-                     "row_min_passed_slots": c["row_min_passed_slots"],
                      "lane_efficiency": useful / max(c["exp_block_lanes"], 1)},
             "pipes_ncu": pipes,
             "hbm": {"volume_gbs": vol_bytes / ((fwd_ms + bwd_ms) * 1e-3) / 1e9, "peak_gbs": pk.get("hbm_gbs")}}

@@ -148,27 +148,6 @@ __device__ __forceinline__ float row_m(float q22, float a, float b, float e2) {
     return __fmaf_rn(__fmaf_rn(q22, e2, b), e2, a);
 }
 
-// -1 / (4 q22) for row_may_include, or NaN (no claim) when q22 is not positive.
-__device__ __forceinline__ float row_min_coef(float q22) {
-    return q22 > 0.0f ? __fdiv_rn(-0.25f, q22) : __int_as_float(0x7fc00000);
-}
-
-// Conservative row test: false only when no voxel of the row can pass the
-// cutoff, i.e. row_m(q22, A, B, e2) > 9 for every e2.  For q22 > 0 the exact
-// quadratic M(e2) = q22 e2^2 + B e2 + A has its minimum A - B^2 / (4 q22).
-// The FP32 row form is within (18 + |A|) u of M wherever it is <= 9
-// (u = 2^-24: one rounding in each of its two FMAs), and the FP32 minimum
-// below is within (|A| + |min|) 3u + |min| u of the exact one, so a minimum
-// above 9 + 1e-4 (|A| + |min| + 32) -- a guard of a few hundred times both
-// bounds -- rules the row out.  NaN or infinite terms make no claim (the
-// comparison is false).  The inclusion test itself is unchanged: voxels of
-// rows that pass are still decided by row_m <= 9.
-__device__ __forceinline__ bool row_may_include(float neg_inv4q22, float a, float b) {
-    const float mn = __fmaf_rn(__fmul_rn(b, b), neg_inv4q22, a);
-    const float lim = __fmaf_rn(1e-4f, __fadd_rn(fabsf(a), fabsf(mn)), 9.0032f);
-    return !(mn > lim);
-}
-
 // ---------------------------------------------------------------------------
 // Workspace layout.  Both blobs are carved at 256-byte boundaries.
 // ---------------------------------------------------------------------------

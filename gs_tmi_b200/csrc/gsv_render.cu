@@ -318,7 +318,6 @@ __device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, in
     }
     if (bits) {
         const int pos = __popc(keep & ((1u << lane) - 1u));
-        r.pad = row_min_coef(r.q22);  // the staged record carries the row-minimum coefficient
         S.rec[pos] = r;
         S.gid[pos] = gid;
         S.meta[pos] = bits | (lane << 8);
@@ -372,11 +371,15 @@ __device__ __forceinline__ void forward_tile(const RenderArgs& a, int64_t tile, 
                     if (!(bits & (1 << r))) continue;  // slot out of the Gaussian's extent
                     const float e0 = __fsub_rn(ev0[r], g.c0);
                     const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
-                    // the slot runs only if some lane's row can reach the cutoff
-                    if (__any_sync(kFull, row_may_include(g.pad, A, B))) {
-                        float m[8];
+                    float m[8];
+                    bool any = false;
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) m[k] = row_m(g.q22, A, B, e2[k]);
+                    for (int k = 0; k < 8; ++k) {
+                        m[k] = row_m(g.q22, A, B, e2[k]);
+                        any |= (m[k] <= kCut);
+                    }
+                    // the exp / FMA part of the slot runs only if some lane needs it
+                    if (__any_sync(kFull, any)) {
 #pragma unroll
                         for (int k = 0; k < 8; ++k) {
                             if (m[k] <= kCut) {
@@ -516,23 +519,26 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
             // per row: Dr/Di = sum w g_r / g_i; R1/R2 = sum a e2 / a e2^2 with
             // a = w (hr g_r + hi g_i); sum a itself = hr Dr + hi Di (after the loop)
             float e0[RPL], Dr[RPL], Di[RPL], R1[RPL], R2[RPL];
-            bool hit = false;
+            bool wany = false;
 #pragma unroll
             for (int r = 0; r < RPL; ++r) {
                 e0[r] = __fsub_rn(ev0[r], g.c0);
                 Dr[r] = Di[r] = R1[r] = R2[r] = 0.f;
                 if (!(bits & (1 << r))) continue;  // slot out of the Gaussian's extent
                 const float A = row_a(g, e0[r], e1), B = row_b(g, e0[r], e1);
-                // warp-uniform row-slot skip: no lane's row can reach the cutoff
-                if (!__any_sync(kFull, row_may_include(g.pad, A, B))) continue;
                 float m[8];
+                bool any = false;
 #pragma unroll
-                for (int k = 0; k < 8; ++k) m[k] = row_m(g.q22, A, B, e2[k]);
+                for (int k = 0; k < 8; ++k) {
+                    m[k] = row_m(g.q22, A, B, e2[k]);
+                    any |= (m[k] <= kCut);
+                }
+                if (!__any_sync(kFull, any)) continue;  // warp-uniform row-slot skip
+                wany = true;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     const int q = r * 8 + k;
                     if (m[k] <= kCut) {
-                        hit = true;
                         const float wgt = ex2_approx(m[k] * kNegHalfLog2e);
                         Dr[r] = fmaf(wgt, gr[q], Dr[r]);
                         Di[r] = fmaf(wgt, gi[q], Di[r]);
@@ -542,7 +548,7 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
                     }
                 }
             }
-            if (!__any_sync(kFull, hit)) {  // no included voxel here: the pair's partial is zero
+            if (!wany) {  // no included voxel here: the pair's partial is zero
                 if (DET && lane == 0) {
                     float4* dst = reinterpret_cast<float4*>(a.partials + int64_t(S.pidx[j]) * kMomStride);
                     dst[0] = dst[1] = dst[2] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1170,10 +1176,7 @@ __global__ void __launch_bounds__(256) k_gather_det_batched(const BatchTable t) 
 //   out[1]  candidates the kernels evaluate m for (voxels of kept slots),
 //   out[2]  lanes issued by the per-column exp / FMA blocks (32 per column
 //           of a kept slot in which some lane is inside the cutoff),
-//   out[3]  kept slots without any included voxel,
-//   out[4]  kept slots in which some lane's row passes the row-minimum test
-//           (row_may_include), i.e. the slots whose voxels the kernels
-//           evaluate.
+//   out[3]  kept slots without any included voxel.
 // out[0] / out[2] is the lane efficiency of the exp / FMA blocks.  The
 // inclusion count covers every listed slot, culled or not, so it also checks
 // that the cull drops no included voxel.
@@ -1184,15 +1187,14 @@ __global__ void __launch_bounds__(kThreads) k_count_work(const RenderArgs a, uns
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int d0, h0, w0;
     decode_tile(a, tile, d0, h0, w0);
-    unsigned long long c_inc = 0, c_eval = 0, c_lanes = 0, c_empty = 0, c_pass = 0;
+    unsigned long long c_inc = 0, c_eval = 0, c_lanes = 0, c_empty = 0;
     const float ev1 = float(h0 + (lane & 7));
     const bool h_ok = h0 + (lane & 7) < a.h;
     for (int p = rg.x + warp; p < rg.y; p += kWarps) {
         const int gid = __ldg(a.pair_ids + p);
         float ih[3];
         compat_ih<false>(a, ih);
-        Rec g = load_rec<false>(a, gid, ih);
-        g.pad = row_min_coef(g.q22);
+        const Rec g = load_rec<false>(a, gid, ih);
         const float4 x = __ldg(a.ext + gid);
         const bool hw = __fsub_rn(g.c1, x.y) <= float(h0 + 7) && __fadd_rn(g.c1, x.y) >= float(h0) &&
                         __fsub_rn(g.c2, x.z) <= float(w0 + 7) && __fadd_rn(g.c2, x.z) >= float(w0);
@@ -1205,7 +1207,6 @@ __global__ void __launch_bounds__(kThreads) k_count_work(const RenderArgs a, uns
             const int gd = ds + (lane >> 3);
             const float e0 = __fsub_rn(float(gd), g.c0);
             const float A = row_a(g, e0, e1), B = row_b(g, e0, e1);
-            const bool pass = __any_sync(kFull, row_may_include(g.pad, A, B));
             bool slot_any = false;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
@@ -1219,7 +1220,6 @@ __global__ void __launch_bounds__(kThreads) k_count_work(const RenderArgs a, uns
             if (kept) {
                 c_eval += 8;
                 if (!slot_any && lane == 0) c_empty += 1;
-                if (pass && lane == 0) c_pass += 1;
             }
         }
     }
@@ -1229,14 +1229,12 @@ __global__ void __launch_bounds__(kThreads) k_count_work(const RenderArgs a, uns
         c_eval += __shfl_xor_sync(kFull, c_eval, o);
         c_lanes += __shfl_xor_sync(kFull, c_lanes, o);
         c_empty += __shfl_xor_sync(kFull, c_empty, o);
-        c_pass += __shfl_xor_sync(kFull, c_pass, o);
     }
     if (lane == 0) {
         atomicAdd(out, c_inc);
         atomicAdd(out + 1, c_eval);
         atomicAdd(out + 2, c_lanes);
         atomicAdd(out + 3, c_empty);
-        atomicAdd(out + 4, c_pass);
     }
 }
 
@@ -1395,7 +1393,7 @@ int gsv_count_work(gsv_shape shape, int64_t n, const void* ws_gauss, const void*
         return GSV_ERR_INVALID_ARGUMENT;
     if (ntiles > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    GSV_CUDA_TRY(cudaMemsetAsync(out, 0, 5 * sizeof(unsigned long long), st));
+    GSV_CUDA_TRY(cudaMemsetAsync(out, 0, 4 * sizeof(unsigned long long), st));
     if (capacity == 0 || n == 0) return GSV_OK;
     RenderArgs a{};
     fill_shape(a, shape);

@@ -130,16 +130,14 @@ def prepare_and_bin(params: Tuple[torch.Tensor, ...], shape: GsvShape, flags: in
 def work_census(plan: BinPlan, cull: bool = True) -> dict:
     """What the tile-8 render kernels do on a binned problem
     (gsv_count_work): included candidates, candidates evaluated after the
-    extent cull, lanes issued by the exp / FMA blocks, kept slots without
-    an included voxel and kept slots that pass the row-minimum test.
-    Synchronises the current stream."""
-    out = torch.zeros(5, dtype=torch.int64, device=plan.device)
+    extent cull, lanes issued by the exp / FMA blocks and kept slots without
+    an included voxel.  Synchronises the current stream."""
+    out = torch.zeros(4, dtype=torch.int64, device=plan.device)
     tune = _lib.GsvTuning(2, 32, 0 if cull else _lib.GSV_TUNE_NO_CULL)
     check(lib.gsv_count_work(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity or 0,
                              ctypes.byref(tune), _ptr(out), _stream(plan.device)), "gsv_count_work")
-    inc, ev, lanes, empty, passed = (int(x) for x in out.cpu())
-    return {"included": inc, "evaluated": ev, "exp_block_lanes": lanes, "empty_kept_slots": empty,
-            "row_min_passed_slots": passed}
+    inc, ev, lanes, empty = (int(x) for x in out.cpu())
+    return {"included": inc, "evaluated": ev, "exp_block_lanes": lanes, "empty_kept_slots": empty}
 
 
 class _VoxelizeFn(torch.autograd.Function):

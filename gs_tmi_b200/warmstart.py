@@ -219,6 +219,13 @@ class WarmConfig:
     # the training target: "best" = the plain fit's best-PSNR evaluation under the reference
     # trainer's metric-plateau stop (what the reference reports); "last" = its last iterate
     target: str = "best"
+    # MLP seeds per training phantom relative to the plain method's count: the network sets up
+    # the larger Gaussian set the plain method only reaches through densification
+    seed_factor: float = 1.0
+    # training loss: "volume" = relative L2 of the rendered volume to the target volume;
+    # "dc" = the same after hard data consistency of both (only the unsampled k-space, which the
+    # measured samples do not fix, is compared)
+    loss: str = "volume"
 
 
 @dataclass
@@ -229,6 +236,8 @@ class TrainingCase:
     base: synthetic.GaussianSet   # intensity-seeded Gaussians (the plain init)
     scale: float
     target: torch.Tensor          # complex64 volume of the plain fit
+    coils: Optional[torch.Tensor] = None  # (C,D,H,W) complex64, for the "dc" loss
+    mask: Optional[torch.Tensor] = None   # (D,H,W) float32, for the "dc" loss
 
 
 def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device):
@@ -250,19 +259,34 @@ def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
     case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed,
                               mask_kind=wc.mask_kind)
     n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
-    x, vox, base, scale = case_inputs(case, n, seed + 1, device)
+    _, _, plain_base, _ = case_inputs(case, n, seed + 1, device)
+    if wc.seed_factor == 1.0:
+        x, vox, base, scale = case_inputs(case, n, seed + 1, device)
+    else:
+        x, vox, base, scale = case_inputs(case, int(round(n * wc.seed_factor)), seed + 2, device)
     if wc.target == "best":
         cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=50, plateau_stop=True, keep_best=True)
     else:
         cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=10 ** 9)
-    res = sense.fit(case, base, cfg, device=device, eval_ssim=False)
+    res = sense.fit(case, plain_base, cfg, device=device, eval_ssim=False)
     from .tile_voxelizer import TileVoxelizer
 
     vz = TileVoxelizer(wc.shape, device=device)
     g = res.best_params if wc.target == "best" else res.params.snapshot()
     with torch.no_grad():
         target = vz(g.positions, g.scales, g.rotations, torch.complex(g.density_r, g.density_i))
-    return TrainingCase(wc.shape, x, vox, base, scale, target.detach())
+    dev = torch.device(device)
+    coils = case.sensitivity_maps.to(dev).to(torch.complex64) if wc.loss == "dc" else None
+    mask = case.mask.to(dev).float() if wc.loss == "dc" else None
+    return TrainingCase(wc.shape, x, vox, base, scale, target.detach(), coils, mask)
+
+
+def _unsampled(vol: torch.Tensor, coils: torch.Tensor, mask: torch.Tensor) -> torch.Tensor:
+    """The part of `vol` hard data consistency leaves in place: the coil
+    images' k-space outside the sampling mask, combined back with the coils
+    (the difference of two hard-DC volumes is this map of their difference)."""
+    k = synthetic.fft3c(coils * vol.unsqueeze(0)) * (1.0 - mask).unsqueeze(0)
+    return (torch.conj(coils) * synthetic.ifft3c(k)).sum(0)
 
 
 def render_step(mlp: WarmStartMLP, tc: TrainingCase, vox) -> float:
@@ -274,6 +298,8 @@ def render_step(mlp: WarmStartMLP, tc: TrainingCase, vox) -> float:
     pos, scl, rot, dr, di = decode(out, tc.seed_vox, tc.base, tc.shape, tc.scale)
     vol = vox(pos, scl, rot, torch.complex(dr, di))
     diff = vol - tc.target
+    if tc.coils is not None:  # "dc" loss: compare what hard data consistency keeps
+        diff = _unsampled(diff, tc.coils, tc.mask)
     loss = (diff.real.square().sum() + diff.imag.square().sum()) / tc.target.abs().square().sum()
     loss.backward()
     mlp.apply_grads(mlp.backward(cache, out.grad))
@@ -310,7 +336,8 @@ def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed:
 
 
 def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_points: int, seed: int = 0,
-                   device="cuda:0", cadence: int = 10, max_iterations: int = 2000) -> dict:
+                   device="cuda:0", cadence: int = 10, max_iterations: int = 2000,
+                   warm_points: Optional[int] = None, ablation: bool = False) -> dict:
     """Warm start against the plain method on one acquisition.
 
     The plain method runs as the reference trainer runs it (evaluation
@@ -320,7 +347,11 @@ def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_poi
     NMSE first reaches the target, evaluated every `cadence` iterations.
     Times are wall seconds of initialisation plus fitting (evaluations
     excluded); all fits use the deterministic backward, so the plain rerun
-    retraces the first run exactly.  `mlp` None: the warm arm is skipped."""
+    retraces the first run exactly.  `mlp` None: the warm arm is skipped.
+    `warm_points`: seeds of the warm start (default `num_points`);
+    `ablation`: also time intensity seeding with `warm_points` seeds and no
+    network, which separates what the network adds from what the larger
+    seed count adds."""
     dev = torch.device(device)
     shape = tuple(case.ground_truth.shape)
     rule = sense.FitConfig(iterations=max_iterations, eval_every=50, plateau_stop=True, deterministic=True)
@@ -350,14 +381,21 @@ def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_poi
            "plain_seconds_to_target": None if p_s is None else p_s + t_plain_init}
     if mlp is None:
         return row
-    warm, t_warm_init = timed_init(lambda: warm_init(mlp, case, num_points, seed=seed, device=device))
+    nw = warm_points or num_points
+    warm, t_warm_init = timed_init(lambda: warm_init(mlp, case, nw, seed=seed, device=device))
     w = sense.fit(case, warm, to_target, device=device, stop_nmse=target, eval_ssim=False)
     w_it, w_s = first_hit(w)
-    row.update({"warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": w_it,
+    row.update({"warm_points": nw, "warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": w_it,
                 "warm_init_seconds": t_warm_init,
                 "warm_seconds_to_target": None if w_s is None else w_s + t_warm_init})
     if w_s is not None and p_s:
         row["wall_ratio"] = row["warm_seconds_to_target"] / row["plain_seconds_to_target"]
+    if ablation:
+        seeded, t_seed = timed_init(lambda: synthetic.from_image_init(case.zero_filled, nw, seed=seed, device=dev))
+        a = sense.fit(case, seeded, to_target, device=device, stop_nmse=target, eval_ssim=False)
+        a_it, a_s = first_hit(a)
+        row.update({"seeded_nmse_at_0": a.history[0]["nmse"], "seeded_iterations_to_target": a_it,
+                    "seeded_seconds_to_target": None if a_s is None else a_s + t_seed})
     return row
 
 

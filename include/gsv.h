@@ -216,15 +216,13 @@ GSV_API int gsv_backward_ex(const gsv_params* params, gsv_shape shape, void* ws_
 
 /* No counterpart in the reference: a census of the work the tile-8 render
  * kernels do on a binned problem (a diagnostic for the roofline; results
- * unchanged).  out: FIVE device uint64 counters, overwritten --
+ * unchanged).  out: FOUR device uint64 counters, overwritten --
  *   [0] included candidates (Mahalanobis <= 9, voxel inside the volume),
  *   [1] candidates the kernels evaluate the quadratic for (voxels of the
  *       4x8x8 row slots the extent cull keeps),
  *   [2] lanes issued by the per-column exp / FMA blocks (32 per voxel column
  *       of a kept slot in which some lane is inside the cutoff),
- *   [3] kept slots without any included voxel,
- *   [4] kept slots whose voxels the kernels evaluate (some lane's row passes
- *       the conservative row-minimum test).
+ *   [3] kept slots without any included voxel.
  * tuning (may be NULL): only GSV_TUNE_NO_CULL is read.  Tile edge 8 only.
  * Asynchronous on `stream`. */
 GSV_API int gsv_count_work(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs,

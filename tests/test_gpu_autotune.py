@@ -137,9 +137,11 @@ def test_tile4_kernels(kind, cuda_device):
     """The 4^3 kernels (one warp per tile): against the FP64 oracle, and
     bitwise the same with the extent cull on and off.  The anisotropic set
     (scales over four orders of magnitude, random-sign densities) cancels
-    heavily in FP32 sums; there the bar is the 8^3 kernels' own error on
-    the same set (x3: the two kernels round their sums in different
-    orders), instead of the fixed tolerances."""
+    heavily in FP32 sums (gradient errors near 1% for either kernel); there
+    the bar is 4x the 8^3 kernels' own error on the same set, instead of
+    the fixed tolerances: the two kernels round their sums in different
+    orders, and with atomics in a different order on every run, so the ratio
+    of their errors scatters around 1 (3.03 once in about twenty runs)."""
     shape = (37, 48, 30)
     gs = {"random": lambda: synthetic.random_gaussians(3000, shape, seed=91),
           "aniso": lambda: _aniso_set(3000, shape, 92),
@@ -156,8 +158,8 @@ def test_tile4_kernels(kind, cuda_device):
     if kind == "aniso":
         tr8, pid8 = O.build_tile_pairs(c, r, shape, 8)
         v8, g8 = _run(prepare_and_bin(params, _shape(shape, 8)), params, gv.to(cuda_device), GsvTuning(2, 32, 0))
-        fwd_tol = max(FWD_TOL, 3 * rel(v8, O.forward(p, shape, 8, tr8, pid8)[0]))
-        grad_tol = [max(GRAD_TOL, 3 * rel(a, b)) for a, b in zip(g8, O.backward(p, shape, 8, tr8, pid8, gv.numpy()))]
+        fwd_tol = max(FWD_TOL, 4 * rel(v8, O.forward(p, shape, 8, tr8, pid8)[0]))
+        grad_tol = [max(GRAD_TOL, 4 * rel(a, b)) for a, b in zip(g8, O.backward(p, shape, 8, tr8, pid8, gv.numpy()))]
     for flags in (0, GSV_BACKWARD_DETERMINISTIC):
         plan = prepare_and_bin(params, _shape(shape, 4), flags=flags)
         on = _run(plan, params, gv.to(cuda_device), GsvTuning(2, 32, 0))

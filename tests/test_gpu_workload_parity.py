@@ -103,7 +103,7 @@ def test_workload_vs_reference_kernels(name, cuda_device):
         tr, pid = torch_port.build_tile_pairs_torch(center, torch_port.radius_vox(params[1], half), shape, ts)
     dr, di = params[3], params[4]
     g = gv.to(dev)
-    gr, gi = g.real.contiguous(), g.imag.contiguous()
+    gr, gi = g.real.reshape(-1).contiguous(), g.imag.reshape(-1).contiguous()
     rvr, rvi = REF.forward(center, cov_inv, dr, di, tr, pid, half, ts, d, h, w)
     rg = REF.backward(center, cov_inv, dr, di, tr, pid, half, gr, gi, ts, d, h, w)
     ctx_in = [t.detach().clone().requires_grad_(True) for t in (center, cov_inv, dr, di)]
@@ -149,9 +149,13 @@ def test_workload_vs_reference_kernels(name, cuda_device):
     assert res["this_build_forward_vs"]["rowform"] < FWD_TOL
     for k, e in res["this_build_grads_vs_oracle"].items():
         assert e < GRAD_TOL, (k, e)
-    # the reference kernels fit the oracle under the reference's op order at least
-    # as well as under this build's predicate, and the builds differ only by the
-    # flipped candidates (a few in a million)
+    # the oracle under the reference's op order reproduces the reference kernels to FP32 noise
+    # (measured 2.3e-7 / 1.2e-7 with the division as a reciprocal product, the fast-math build),
+    # and the two builds differ only by the flipped candidates: a few in ten million, each moving
+    # one voxel by exp(-4.5)|rho| (measured: volume 8.8e-7 / 5.3e-6, gradients <= 5.4e-5)
+    assert res["ref_kernel_forward_vs"][best] < 1e-6
     assert res["ref_kernel_forward_vs"][best] <= res["ref_kernel_forward_vs"]["rowform"]
     assert res["flips_vs_rowform"][best] <= 1e-5 * res["included"]["rowform"]
-    assert res["this_build_vs_ref_kernel"]["forward"] < 2e-3
+    assert res["this_build_vs_ref_kernel"]["forward"] < 1e-4
+    for k in names:
+        assert res["this_build_vs_ref_kernel"][k] < 5e-4, k
