@@ -258,33 +258,46 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
         if (w < warp) warp_base += warp_tot[w];
         block_tot += warp_tot[w];
     }
-    if (threadIdx.x == 0) {
+    if (warp == 0) {
+        // Look-back by the whole first warp: lane l reads the word of block j - l, so one
+        // step covers 32 predecessors.  The nearest inclusive prefix (kLbPre) in the window
+        // ends the walk; every word in front of it must be published (flag set) before the
+        // window is summed, else the step is retried (bounded).
         unsigned long long* lb = reinterpret_cast<unsigned long long*>(status + 1);
         int64_t base = 0;
         if (bid == 0) {
-            lb_store(&lb[0], kLbPre | (unsigned long long)block_tot);
+            if (lane == 0) lb_store(&lb[0], kLbPre | (unsigned long long)block_tot);
         } else {
-            lb_store(&lb[bid], kLbAgg | (unsigned long long)block_tot);
-            int64_t j = bid - 1;
+            if (lane == 0) lb_store(&lb[bid], kLbAgg | (unsigned long long)block_tot);
+            int64_t j = bid - 1;  // the window's nearest predecessor
             int spins = 0;
             while (true) {
-                const unsigned long long v = lb_load(&lb[j]);
+                const int64_t idx = j - lane;
+                // before block 0 there is nothing: an inclusive prefix of zero
+                const unsigned long long v = idx >= 0 ? lb_load(&lb[idx]) : kLbPre;
                 const unsigned long long f = v & ~kLbVal;
-                if (f == 0) {
+                const unsigned pre = __ballot_sync(0xffffffffu, f == kLbPre);
+                const int first = pre ? __ffs(pre) - 1 : 31;        // last lane of this step
+                const unsigned upto = first == 31 ? 0xffffffffu : (2u << first) - 1u;
+                const unsigned missing = __ballot_sync(0xffffffffu, f == 0) & upto;
+                if (missing) {
                     if (++spins > kLbSpinLimit) {
-                        atomicOr(&status->flags, GSV_FLAG_SCAN_STALLED);
+                        if (lane == 0) atomicOr(&status->flags, GSV_FLAG_SCAN_STALLED);
                         break;
                     }
                     continue;
                 }
                 spins = 0;
-                base += int64_t(v & kLbVal);
-                if (f == kLbPre || j == 0) break;
-                --j;
+                int64_t part = ((upto >> lane) & 1u) ? int64_t(v & kLbVal) : 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                base += part;
+                if (pre) break;
+                j -= 32;
             }
-            lb_store(&lb[bid], kLbPre | (unsigned long long)(base + block_tot));
+            if (lane == 0) lb_store(&lb[bid], kLbPre | (unsigned long long)(base + block_tot));
         }
-        block_base = base;
+        if (lane == 0) block_base = base;
     }
     __syncthreads();
     if (g <= n) offsets[g] = block_base + warp_base + incl - cnt;
