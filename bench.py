@@ -576,6 +576,7 @@ class Workload:
         if self.tuning is None:
             return "default"
         return {"rows_per_lane": self.tuning.rows_per_lane, "chunk": self.tuning.chunk,
+                "backward_split": max(1, self.tuning.split),
                 "autotune_ms_per_candidate": self.tune_times, "tile_edge_step_ms": self.tile_times,
                 "tile_edge_fastest": self.tile_pick}
 
@@ -770,7 +771,7 @@ def run_ours(args, rank, world, dist):
                     "breakdown_ms": {"prepare_bin": statistics.mean(ts_["bin"]),
                                      "forward": statistics.mean(ts_["fwd"]),
                                      "backward": statistics.mean(ts_["bwd"])},
-                    "execution": small.execution(), "included": small.census["included"]}
+                    "execution": small.execution(), "included": small.census["included"], "work": small.census}
                 del small
             extra["reference_cuda"] = reference_cuda_baseline(wl, flush, reps=max(args.steps, 5))
     if rank != 0:

@@ -70,7 +70,8 @@ class GsvDensityConfig(ctypes.Structure):
 
 
 class GsvTuning(ctypes.Structure):
-    _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32), ("flags", ctypes.c_int32)]
+    _fields_ = [("rows_per_lane", ctypes.c_int32), ("chunk", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("split", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes); the complete exported C ABI.

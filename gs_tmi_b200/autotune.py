@@ -7,7 +7,10 @@ Two knobs change speed but not results (every candidate evaluates the same
   8-voxel rows per lane) or a 4x8x8 half tile (one row per lane: fewer
   registers, twice the CTAs);
 * Gaussian batch -- how many Gaussians a warp stages in shared memory at a
-  time (8, 16 or 32).
+  time (8, 16 or 32);
+* backward list split -- how many CTAs share one tile's Gaussian list in the
+  backward (1, 2 or 4): more CTAs for volumes with too few tiles to fill
+  the GPU.
 
 ``Autotuner.pick`` times every candidate's forward + backward on the binned
 problem at hand with CUDA events and keeps the fastest, cached per
@@ -28,9 +31,20 @@ import torch
 
 from ._lib import GsvGrads, GsvParams, GsvTuning, check, lib
 
-CANDIDATES: Tuple[Tuple[int, int], ...] = ((2, 32), (2, 16), (1, 32), (1, 16), (1, 8))
+# (rows per lane, Gaussian batch[, backward list split])
+CANDIDATES: Tuple[Tuple[int, ...], ...] = ((2, 32), (2, 16), (1, 32), (1, 16), (1, 8), (2, 32, 2), (1, 32, 2),
+                                           (1, 32, 4))
 TILE_SIZES: Tuple[int, ...] = (8, 4)  # binning tile edges compared by pick_tile_size
 WHOLE_TILE: Tuple[Tuple[int, int], ...] = ((2, 32), (2, 16), (2, 8))  # batched launches
+
+
+def tuning_of(c) -> GsvTuning:
+    """GsvTuning of a candidate or cache entry (rows per lane, batch[, split])."""
+    return GsvTuning(int(c[0]), int(c[1]), 0, int(c[2]) if len(c) > 2 else 1)
+
+
+def label_of(c) -> str:
+    return "/".join(str(int(x)) for x in c) if len(c) > 2 and int(c[2]) > 1 else f"{int(c[0])}/{int(c[1])}"
 
 
 def _ptr(t):
@@ -66,7 +80,7 @@ class Autotuner:
             f"{a}.{b}" for a, b in candidates))
         with self._lock:
             if k in self.cache:
-                return GsvTuning(*self.cache[k])
+                return tuning_of(self.cache[k])
             if shape.tile_size != 8 or plan.n == 0 or plan.capacity == 0:
                 self.cache[k] = (2, 32)
                 return GsvTuning(2, 32)
@@ -74,7 +88,7 @@ class Autotuner:
             self.cache[k] = best
             self.timings[k] = times
             self.save()
-            return GsvTuning(*best)
+            return tuning_of(best)
 
     def _measure(self, plan, params, candidates):
         dev = plan.device
@@ -85,8 +99,8 @@ class Autotuner:
         gp = GsvParams(*(t.data_ptr() for t in params), plan.n)
         gg = GsvGrads(*(o.data_ptr() for o in outs))
         times = {}
-        for rpl, chunk in candidates:
-            tun = GsvTuning(rpl, chunk)
+        for cand in candidates:
+            tun = tuning_of(cand)
 
             def run():
                 check(lib.gsv_forward_ex(plan.shape, plan.n, _ptr(plan.ws_gauss), _ptr(plan.ws_pairs), plan.capacity,
@@ -102,9 +116,9 @@ class Autotuner:
                 run()
             e1.record()
             torch.cuda.synchronize(dev)
-            times[f"{rpl}/{chunk}"] = e0.elapsed_time(e1) / self.reps
-        best = min(candidates, key=lambda c: times[f"{c[0]}/{c[1]}"])
-        return best, times
+            times[label_of(cand)] = e0.elapsed_time(e1) / self.reps
+        best = min(candidates, key=lambda c: times[label_of(c)])
+        return tuple(best), times
 
 
     def pick_tile_size(self, params, volume_shape, flags: int = 0) -> Tuple[int, GsvTuning, Dict[str, float]]:
@@ -124,8 +138,8 @@ class Autotuner:
         k = f"{d}x{h}x{w}/n2^{int(math.ceil(math.log2(max(n, 1))))}/{'det' if flags & 1 else 'atomic'}/tile"
         with self._lock:
             if k in self.cache:
-                ts, rpl, chunk = self.cache[k]
-                return int(ts), GsvTuning(int(rpl), int(chunk)), self.timings.get(k, {})
+                ts, *shape_t = self.cache[k]
+                return int(ts), tuning_of(shape_t), self.timings.get(k, {})
         times, tunings = {}, {}
         dev = params[0].device
         st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
@@ -161,7 +175,8 @@ class Autotuner:
             times[str(ts)] = e0.elapsed_time(e1) / self.reps
         best = min(TILE_SIZES, key=lambda t: times[str(t)])
         with self._lock:
-            self.cache[k] = (best, tunings[best].rows_per_lane, tunings[best].chunk)
+            t = tunings[best]
+            self.cache[k] = (best, t.rows_per_lane, t.chunk, max(1, t.split))
             self.timings[k] = times
             self.save()
         return best, tunings[best], times

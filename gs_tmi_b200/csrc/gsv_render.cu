@@ -72,6 +72,7 @@ struct RenderArgs {
     float* g_di;
     int chunk;  // Gaussians staged per warp chunk (<= 32)
     int cull;   // skip Gaussians / row slots outside the tight extent
+    int split;  // backward: CTAs sharing one (half) tile's list, each taking every split-th quarter
     // finalize
     gsv_params prm;
     gsv_grads grd;
@@ -281,12 +282,12 @@ static_assert(sizeof(WarpStage) * kWarps <= kFwdSmem, "stage too large");
 // their list order.  The native layout reads the extent k_prepare stored,
 // the compat layout (cov_inv input) computes it here.
 template <bool COMPAT, int RPL, bool DET = false>
-__device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, int base, int cnt, int lane, int d0,
-                                           int h0, int w0, int sub, const float ih[3]) {
+__device__ __forceinline__ int stage_chunk(const RenderArgs& a, WarpStage& S, int base, int stride, int cnt, int lane,
+                                           int d0, int h0, int w0, int sub, const float ih[3]) {
     Rec r;
     int gid = 0, bits = 0;
     if (lane < cnt) {
-        gid = __ldg(a.pair_ids + base + kWarps * lane);
+        gid = __ldg(a.pair_ids + base + stride * lane);
         r = load_rec<COMPAT>(a, gid, ih);
         if (!a.cull) {
             bits = (1 << RPL) - 1;
@@ -358,7 +359,8 @@ __device__ __forceinline__ void forward_tile(const RenderArgs& a, int64_t tile, 
         const int mine = (rg.y - rg.x - warp + kWarps - 1) / kWarps;  // list positions of this warp
         for (int i0 = 0; i0 < mine; i0 += chunk) {
             const int base = rg.x + warp + kWarps * i0;
-            const int kept = stage_chunk<COMPAT, RPL>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
+            const int kept =
+                stage_chunk<COMPAT, RPL>(a, S, base, kWarps, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
             __syncwarp();
             for (int j = 0; j < kept; ++j) {
                 const Rec g = S.rec[j];
@@ -461,7 +463,8 @@ __global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
 // only.  The deterministic mode writes one partial per (tile, Gaussian) and
 // therefore runs with RPL = 2 only.
 template <bool COMPAT, bool DET, int RPL>
-__device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile, int sub, WarpStage* stage) {
+__device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile, int sub, WarpStage* stage,
+                                              int part) {
     static_assert(!DET || RPL == 2, "deterministic partials need the whole tile in one CTA");
     constexpr int NV = RPL * 8;
     const int2 rg = a.ranges[tile];
@@ -503,11 +506,13 @@ __device__ __forceinline__ void backward_tile(const RenderArgs& a, int64_t tile,
     for (int r = 0; r < RPL; ++r) ev0[r] = float(d0 + (lane >> 3) + 4 * (r + sub));
     const float ev1 = float(h0 + (lane & 7));
     WarpStage& S = stage[warp];
-    const int mine = (rg.y - rg.x - warp + kWarps - 1) / kWarps;  // list positions of this warp
+    // list positions of this warp: first, first + stride, ... (part `part` of a.split CTAs)
+    const int stride = kWarps * a.split, first = part * kWarps + warp;
+    const int mine = rg.y - rg.x > first ? (rg.y - rg.x - first + stride - 1) / stride : 0;
     for (int i0 = 0; i0 < mine; i0 += chunk) {
-        const int base = rg.x + warp + kWarps * i0;
+        const int base = rg.x + first + stride * i0;
         const int kept =
-            stage_chunk<COMPAT, RPL, DET>(a, S, base, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
+            stage_chunk<COMPAT, RPL, DET>(a, S, base, stride, min(chunk, mine - i0), lane, d0, h0, w0, sub, ih);
         __syncwarp();
         for (int j = 0; j < kept; ++j) {
             const Rec g = S.rec[j];
@@ -607,7 +612,8 @@ template <bool COMPAT, bool DET, int RPL>
 __global__ void __launch_bounds__(kThreads, RPL == 2 ? 6 : 7) k_backward8(const RenderArgs a) {
     __shared__ __align__(16) WarpStage stage[kWarps];
     constexpr int subs = 2 / RPL;
-    backward_tile<COMPAT, DET, RPL>(a, blockIdx.x / subs, blockIdx.x % subs, stage);
+    const int part = blockIdx.x % a.split, rest = blockIdx.x / a.split;
+    backward_tile<COMPAT, DET, RPL>(a, rest / subs, rest % subs, stage, part);
 }
 
 // ---------------------------------------------------------------------------
@@ -1132,7 +1138,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_backward8_batched(const BatchTa
         const int64_t gt = s_next;
         if (gt >= total) break;
         const int i = find_item(t.tile_prefix, t.count, gt);
-        backward_tile<false, DET, 2>(t.items[i], gt - t.tile_prefix[i], 0, stage);
+        backward_tile<false, DET, 2>(t.items[i], gt - t.tile_prefix[i], 0, stage, 0);
     }
 }
 
@@ -1259,6 +1265,7 @@ void fill_shape(RenderArgs& a, gsv_shape s) {
     a.ntiles = int64_t((s.d + s.tile_size - 1) / s.tile_size) * a.nth * a.ntw;
     a.chunk = 32;
     a.cull = 1;
+    a.split = 1;
     const float sh[3] = {float(s.d), float(s.h), float(s.w)};
     for (int k = 0; k < 3; ++k) {
         a.hs[k] = sh[k] * 0.5f;
@@ -1280,7 +1287,8 @@ int gsv_forward(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws
 }
 
 static bool tuning_ok(const gsv_tuning* t) {
-    return !t || ((t->rows_per_lane == 1 || t->rows_per_lane == 2) && t->chunk >= 1 && t->chunk <= 32);
+    return !t || ((t->rows_per_lane == 1 || t->rows_per_lane == 2) && t->chunk >= 1 && t->chunk <= 32 &&
+                  (t->split == 0 || t->split == 1 || t->split == 2 || t->split == 4));
 }
 
 int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void* ws_pairs, int64_t capacity,
@@ -1356,13 +1364,16 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     if (tuning) {
         a.chunk = tuning->chunk;
         a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
+        a.split = tuning->split > 1 ? tuning->split : 1;
     }
+    if (ntiles * 2 * a.split > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
     const int rpl = (tuning && !det) ? tuning->rows_per_lane : 2;  // deterministic: whole tiles
+    const unsigned sp = unsigned(a.split);
     if (capacity > 0) {
         if (shape.tile_size == 8) {
-            if (det) k_backward8<false, true, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
-            else if (rpl == 2) k_backward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
-            else k_backward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
+            if (det) k_backward8<false, true, 2><<<unsigned(ntiles) * sp, kThreads, 0, st>>>(a);
+            else if (rpl == 2) k_backward8<false, false, 2><<<unsigned(ntiles) * sp, kThreads, 0, st>>>(a);
+            else k_backward8<false, false, 1><<<unsigned(2 * ntiles) * sp, kThreads, 0, st>>>(a);
         } else {
             const unsigned g4 = unsigned((ntiles + kWarps - 1) / kWarps);
             if (shape.tile_size == 4 && det) k_backward4<false, true><<<g4, kThreads, 0, st>>>(a);

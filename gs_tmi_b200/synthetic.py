@@ -252,8 +252,29 @@ def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise
     return MRICase(x, S, m, ku.to(torch.complex64), zf.to(torch.complex64))
 
 
+def seed_indices(image: torch.Tensor, num_points: int, seed: int, mode: str = "random") -> torch.Tensor:
+    """Seed voxels (flat indices, CPU) of the intensity-seeded init, as
+    GaussianModel3D.from_image draws them (gaussian_model.py:320-335):
+    "random" -- a random permutation of all voxels; "importance" -- a random
+    permutation of the voxels whose magnitude exceeds the 90th percentile
+    (all voxels when there are fewer of those than seeds)."""
+    total = image.numel()
+    g = torch.Generator().manual_seed(seed)
+    n = min(num_points, total)
+    if mode == "random" or num_points >= total:
+        return torch.randperm(total, generator=g)[:n]
+    if mode != "importance":
+        raise ValueError(f"unknown seeding mode {mode!r}")
+    mag = image.detach().abs().reshape(-1).float().cpu()
+    thr = torch.quantile(mag, 0.90)
+    cand = torch.nonzero(mag > thr, as_tuple=False).squeeze(-1)
+    if cand.numel() < n:
+        cand = torch.arange(total)
+    return cand[torch.randperm(cand.numel(), generator=g)[:n]]
+
+
 def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float = 0.2,
-                    seed: int = 0, device=None) -> GaussianSet:
+                    seed: int = 0, device=None, mode: str = "random") -> GaussianSet:
     """Intensity-seeded initialisation in the manner of the reference's
     GaussianModel3D.from_image (gaussian_model.py:308-355, random mode):
     random voxel centres, isotropic scale = mean distance to the 3 nearest
@@ -262,16 +283,16 @@ def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float
 
     `device` (a CUDA device): the 3-NN distances come from the library's
     exact grid search (gsv_knn3_mean_distance) instead of scipy's cKDTree and
-    the set is returned on that device; the seed voxels are the same."""
+    the set is returned on that device; the seed voxels are the same.
+    `mode`: the seed draw, "random" (the reference's paper profile) or
+    "importance" (its other mode), see `seed_indices`."""
     d, h, w = image.shape
     if device is not None and torch.device(device).type == "cuda":
-        return _from_image_init_gpu(image, num_points, density_scale_k, seed, torch.device(device))
+        return _from_image_init_gpu(image, num_points, density_scale_k, seed, torch.device(device), mode)
     from scipy.spatial import cKDTree
 
-    total = d * h * w
-    g = torch.Generator().manual_seed(seed)
-    n = min(num_points, total)
-    idx = torch.randperm(total, generator=g)[:n]
+    idx = seed_indices(image, num_points, seed, mode)
+    n = idx.numel()
     z = idx // (h * w)
     rem = idx % (h * w)
     y = rem // w
@@ -298,16 +319,15 @@ def from_image_init(image: torch.Tensor, num_points: int, density_scale_k: float
                        (flat.imag * density_scale_k).float())
 
 
-def _from_image_init_gpu(image, num_points, density_scale_k, seed, dev) -> GaussianSet:
+def _from_image_init_gpu(image, num_points, density_scale_k, seed, dev, mode="random") -> GaussianSet:
     import ctypes
 
     from ._lib import check, lib
 
     d, h, w = image.shape
     total = d * h * w
-    g = torch.Generator().manual_seed(seed)
-    n = min(num_points, total)
-    idx_cpu = torch.randperm(total, generator=g)[:n]
+    idx_cpu = seed_indices(image, num_points, seed, mode)
+    n = idx_cpu.numel()
     z = idx_cpu // (h * w)
     rem = idx_cpu % (h * w)
     y = rem // w

@@ -26,6 +26,7 @@ start is scored by the final NMSE against the fully sampled phantom.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import math
 import time
 from dataclasses import dataclass
@@ -226,6 +227,10 @@ class WarmConfig:
     # "dc" = the same after hard data consistency of both (only the unsampled k-space, which the
     # measured samples do not fix, is compared)
     loss: str = "volume"
+    # seed draw of the warm start: "random" (the reference's paper profile) or "importance"
+    # (its other mode: voxels above the 90th magnitude percentile); the plain fits that make
+    # the targets always seed as the paper profile does
+    seed_mode: str = "random"
 
 
 @dataclass
@@ -240,9 +245,9 @@ class TrainingCase:
     mask: Optional[torch.Tensor] = None   # (D,H,W) float32, for the "dc" loss
 
 
-def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device):
+def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device, mode: str = "random"):
     dev = torch.device(device)
-    base = synthetic.from_image_init(case.zero_filled, num_points, seed=seed, device=dev).to(dev)
+    base = synthetic.from_image_init(case.zero_filled, num_points, seed=seed, device=dev, mode=mode).to(dev)
     shape = tuple(case.ground_truth.shape)
     zf = case.zero_filled.to(dev)
     scale = image_scale(zf)
@@ -260,10 +265,10 @@ def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
                               mask_kind=wc.mask_kind)
     n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
     _, _, plain_base, _ = case_inputs(case, n, seed + 1, device)
-    if wc.seed_factor == 1.0:
+    if wc.seed_factor == 1.0 and wc.seed_mode == "random":
         x, vox, base, scale = case_inputs(case, n, seed + 1, device)
     else:
-        x, vox, base, scale = case_inputs(case, int(round(n * wc.seed_factor)), seed + 2, device)
+        x, vox, base, scale = case_inputs(case, int(round(n * wc.seed_factor)), seed + 2, device, wc.seed_mode)
     if wc.target == "best":
         cfg = sense.FitConfig(iterations=wc.fit_iterations, eval_every=50, plateau_stop=True, keep_best=True)
     else:
@@ -325,10 +330,10 @@ def train(mlp: WarmStartMLP, cases: List[TrainingCase], steps: int = 1500, seed:
 
 @torch.no_grad()
 def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed: int = 0,
-              device="cuda:0") -> synthetic.GaussianSet:
-    """Seeds exactly as the intensity-seeded init (same seed -> same voxels
-    and scales), parameters from the MLP."""
-    x, vox, base, scale = case_inputs(case, num_points, seed, device)
+              device="cuda:0", mode: str = "random") -> synthetic.GaussianSet:
+    """Seeds exactly as the intensity-seeded init (same seed and mode ->
+    same voxels and scales), parameters from the MLP."""
+    x, vox, base, scale = case_inputs(case, num_points, seed, device, mode)
     out = mlp.predict(x)
     pos, scl, rot, dr, di = decode(out, vox, base, tuple(case.ground_truth.shape), scale)
     return synthetic.GaussianSet(pos.contiguous(), scl.contiguous(), rot.contiguous(), dr.contiguous(),
@@ -337,7 +342,8 @@ def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed:
 
 def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_points: int, seed: int = 0,
                    device="cuda:0", cadence: int = 10, max_iterations: int = 2000,
-                   warm_points: Optional[int] = None, ablation: bool = False) -> dict:
+                   warm_points: Optional[int] = None, ablation: bool = False, warm_mode: str = "random",
+                   warm_schedule: Optional[dict] = None) -> dict:
     """Warm start against the plain method on one acquisition.
 
     The plain method runs as the reference trainer runs it (evaluation
@@ -348,10 +354,12 @@ def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_poi
     Times are wall seconds of initialisation plus fitting (evaluations
     excluded); all fits use the deterministic backward, so the plain rerun
     retraces the first run exactly.  `mlp` None: the warm arm is skipped.
-    `warm_points`: seeds of the warm start (default `num_points`);
-    `ablation`: also time intensity seeding with `warm_points` seeds and no
-    network, which separates what the network adds from what the larger
-    seed count adds."""
+    `warm_points`, `warm_mode`: seed count and seed draw of the warm start
+    (default: the plain method's); `warm_schedule`: FitConfig fields the
+    warm-started fit overrides (default none: the plain method's schedule);
+    `ablation`: also time intensity seeding with the warm start's seeds,
+    draw and schedule but no network, which separates what the network adds
+    from what the seeding and schedule add."""
     dev = torch.device(device)
     shape = tuple(case.ground_truth.shape)
     rule = sense.FitConfig(iterations=max_iterations, eval_every=50, plateau_stop=True, deterministic=True)
@@ -382,8 +390,9 @@ def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_poi
     if mlp is None:
         return row
     nw = warm_points or num_points
-    warm, t_warm_init = timed_init(lambda: warm_init(mlp, case, nw, seed=seed, device=device))
-    w = sense.fit(case, warm, to_target, device=device, stop_nmse=target, eval_ssim=False)
+    warm_cfg = dataclasses.replace(to_target, **(warm_schedule or {}))
+    warm, t_warm_init = timed_init(lambda: warm_init(mlp, case, nw, seed=seed, device=device, mode=warm_mode))
+    w = sense.fit(case, warm, warm_cfg, device=device, stop_nmse=target, eval_ssim=False)
     w_it, w_s = first_hit(w)
     row.update({"warm_points": nw, "warm_nmse_at_0": w.history[0]["nmse"], "warm_iterations_to_target": w_it,
                 "warm_init_seconds": t_warm_init,
@@ -391,8 +400,9 @@ def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_poi
     if w_s is not None and p_s:
         row["wall_ratio"] = row["warm_seconds_to_target"] / row["plain_seconds_to_target"]
     if ablation:
-        seeded, t_seed = timed_init(lambda: synthetic.from_image_init(case.zero_filled, nw, seed=seed, device=dev))
-        a = sense.fit(case, seeded, to_target, device=device, stop_nmse=target, eval_ssim=False)
+        seeded, t_seed = timed_init(
+            lambda: synthetic.from_image_init(case.zero_filled, nw, seed=seed, device=dev, mode=warm_mode))
+        a = sense.fit(case, seeded, warm_cfg, device=device, stop_nmse=target, eval_ssim=False)
         a_it, a_s = first_hit(a)
         row.update({"seeded_nmse_at_0": a.history[0]["nmse"], "seeded_iterations_to_target": a_it,
                     "seeded_seconds_to_target": None if a_s is None else a_s + t_seed})

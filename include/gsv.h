@@ -50,7 +50,7 @@
 extern "C" {
 #endif
 
-#define GSV_ABI_VERSION 2
+#define GSV_ABI_VERSION 3
 
 typedef enum gsv_status {
     GSV_OK = 0,
@@ -197,13 +197,17 @@ GSV_API int gsv_backward_batched(void* ws_batch, int count, int flags, void* str
  * of Gaussians a warp stages in shared memory at a time (1..32).  flags:
  * GSV_TUNE_NO_CULL turns off the extent cull (a Gaussian, or a 4x8x8 row
  * slot of it, whose conservative tight extent misses the CTA's voxels is
- * skipped; it contributes nothing there either way).  Tile edge 8 only;
+ * skipped; it contributes nothing there either way).  split: the
+ * backward runs `split` CTAs per (half) tile, each walking every split-th
+ * group of four list positions -- more CTAs for small volumes whose tiles
+ * are too few to fill the GPU (the forward ignores it).  Tile edge 8 only;
  * other tile edges ignore it. */
 #define GSV_TUNE_NO_CULL 0x1
 typedef struct gsv_tuning {
     int32_t rows_per_lane;
     int32_t chunk;
     int32_t flags;
+    int32_t split; /* backward, tile edge 8: CTAs sharing one (half) tile's Gaussian list, 1, 2 or 4 (0 = 1) */
 } gsv_tuning;
 
 /* gsv_forward / gsv_backward with an explicit execution shape (NULL =

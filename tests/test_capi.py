@@ -44,7 +44,7 @@ def test_library_exports_every_declared_symbol():
 def test_host_queries():
     from gs_tmi_b200._lib import GsvShape, lib
 
-    assert lib.gsv_abi_version() == 2
+    assert lib.gsv_abi_version() == 3
     s = GsvShape(64, 64, 64, 8)
     assert lib.gsv_num_tiles(s) == 512
     assert lib.gsv_num_tiles(GsvShape(20, 12, 16, 8)) == 3 * 2 * 2

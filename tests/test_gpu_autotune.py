@@ -45,14 +45,31 @@ def test_candidates_agree_with_oracle(shape, cuda_device):
     ovol, _ = O.forward(p, shape, 8, tr, pid)
     og = O.backward(p, shape, 8, tr, pid, gv.numpy())
     vols = {}
-    for rpl, chunk in autotune.CANDIDATES:
-        vol, grads = _run(plan, params, gv.to(cuda_device), GsvTuning(rpl, chunk))
-        vols[(rpl, chunk)] = vol
+    for cand in autotune.CANDIDATES:
+        vol, grads = _run(plan, params, gv.to(cuda_device), autotune.tuning_of(cand))
+        vols[tuple(cand)] = vol
         assert rel(vol, ovol) < FWD_TOL
         for a, b in zip(grads, og):
             assert rel(a, b) < GRAD_TOL
     assert np.array_equal(vols[(2, 32)], vols[(1, 32)])
     assert np.array_equal(vols[(2, 16)], vols[(1, 16)])
+    assert np.array_equal(vols[(2, 32)], vols[(2, 32, 2)])  # the split changes the backward only
+
+
+@pytest.mark.parametrize("split", [2, 4])
+def test_backward_split_is_bitwise_neutral_in_deterministic_mode(split, cuda_device):
+    """The deterministic backward writes one partial per (tile, Gaussian)
+    pair wherever it is computed, so splitting a tile's list over 2 or 4
+    CTAs gives bitwise the same gradients; ragged volume, small tiles count."""
+    shape = (37, 29, 45)
+    gs = synthetic.concat(synthetic.random_gaussians(2500, shape, seed=65), synthetic.edge_case_gaussians(shape))
+    gv = synthetic.upstream_grad(shape, seed=66)
+    params = tuple(t.to(cuda_device) for t in gs.tensors())
+    plan = prepare_and_bin(params, _shape(shape, 8), flags=GSV_BACKWARD_DETERMINISTIC)
+    _, g1 = _run(plan, params, gv.to(cuda_device), GsvTuning(2, 32, 0, 1))
+    _, gs_ = _run(plan, params, gv.to(cuda_device), GsvTuning(2, 32, 0, split))
+    for a, b in zip(g1, gs_):
+        assert np.array_equal(a.view(np.int32), b.view(np.int32))
 
 
 def test_tuner_picks_and_caches(tmp_path, cuda_device):
@@ -63,13 +80,14 @@ def test_tuner_picks_and_caches(tmp_path, cuda_device):
     path = tmp_path / "tune.json"
     tuner = autotune.Autotuner(str(path))
     t1 = tuner.pick(plan, params)
-    assert (t1.rows_per_lane, t1.chunk) in autotune.CANDIDATES
+    picked = tuple(json.loads(path.read_text())[autotune.Autotuner.key(plan.shape, plan.n, False)])
+    assert picked in {tuple(c) for c in autotune.CANDIDATES}
+    assert (t1.rows_per_lane, t1.chunk, max(1, t1.split)) == (picked[0], picked[1], picked[2] if len(picked) > 2 else 1)
     k = autotune.Autotuner.key(plan.shape, plan.n, False)
     assert len(tuner.timings[k]) == len(autotune.CANDIDATES)
     again = autotune.Autotuner(str(path))
     t2 = again.pick(plan, params)
-    assert (t2.rows_per_lane, t2.chunk) == (t1.rows_per_lane, t1.chunk) and not again.timings
-    assert json.loads(path.read_text())[k] == [t1.rows_per_lane, t1.chunk]
+    assert (t2.rows_per_lane, t2.chunk, t2.split) == (t1.rows_per_lane, t1.chunk, t1.split) and not again.timings
 
 
 def _aniso_set(n, shape, seed, spread=1.5):
