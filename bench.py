@@ -723,11 +723,12 @@ def run_ours(args, rank, world, dist):
 
         def e2e_step():
             # copies overlap compute the way a caller with two copy streams would run it:
-            # the upstream gradient (independent of this step's parameters) uploads from the
-            # start of the step, during the parameter upload, binning and forward; the volume
-            # downloads during the backward
+            # the upstream gradient uploads during binning + forward, the volume downloads
+            # during the backward (starting the gradient upload with the step, beside the
+            # parameter upload, measured slower: 0.896 -> 0.959 ms per step)
             main = torch.cuda.current_stream(dev)
             ps = [x.to(dev, non_blocking=True).requires_grad_(True) for x in host_in]
+            up.wait_stream(main)
             with torch.cuda.stream(up):
                 g = gv_host.to(dev, non_blocking=True)
             v = vox(ps[0], ps[1], ps[2], torch.complex(ps[3], ps[4]))
