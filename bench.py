@@ -724,8 +724,7 @@ def run_ours(args, rank, world, dist):
         def e2e_step():
             # copies overlap compute the way a caller with two copy streams would run it:
             # the upstream gradient uploads during binning + forward, the volume downloads
-            # during the backward (starting the gradient upload with the step, beside the
-            # parameter upload, measured slower: 0.896 -> 0.959 ms per step)
+            # during the backward
             main = torch.cuda.current_stream(dev)
             ps = [x.to(dev, non_blocking=True).requires_grad_(True) for x in host_in]
             up.wait_stream(main)

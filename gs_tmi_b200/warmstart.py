@@ -222,15 +222,15 @@ class WarmConfig:
     target: str = "best"
     # MLP seeds per training phantom relative to the plain method's count: the network sets up
     # the larger Gaussian set the plain method only reaches through densification
-    seed_factor: float = 1.0
+    seed_factor: float = 3.0
     # training loss: "volume" = relative L2 of the rendered volume to the target volume;
     # "dc" = the same after hard data consistency of both (only the unsampled k-space, which the
     # measured samples do not fix, is compared)
-    loss: str = "volume"
+    loss: str = "dc"
     # seed draw of the warm start: "random" (the reference's paper profile) or "importance"
     # (its other mode: voxels above the 90th magnitude percentile); the plain fits that make
     # the targets always seed as the paper profile does
-    seed_mode: str = "random"
+    seed_mode: str = "importance"
 
 
 @dataclass
@@ -338,6 +338,15 @@ def warm_init(mlp: WarmStartMLP, case: synthetic.MRICase, num_points: int, seed:
     pos, scl, rot, dr, di = decode(out, vox, base, tuple(case.ground_truth.shape), scale)
     return synthetic.GaussianSet(pos.contiguous(), scl.contiguous(), rot.contiguous(), dr.contiguous(),
                                  di.contiguous())
+
+
+def warm_start(mlp: WarmStartMLP, case: synthetic.MRICase, plain_points: int, wc: WarmConfig, seed: int = 0,
+               device="cuda:0") -> synthetic.GaussianSet:
+    """The warm start for an acquisition whose plain fit seeds `plain_points`
+    Gaussians: `wc.seed_factor` times as many seeds, drawn as `wc.seed_mode`,
+    with their parameters from the network."""
+    return warm_init(mlp, case, int(round(plain_points * wc.seed_factor)), seed=seed, device=device,
+                     mode=wc.seed_mode)
 
 
 def time_to_target(mlp: Optional[WarmStartMLP], case: synthetic.MRICase, num_points: int, seed: int = 0,
