@@ -252,12 +252,17 @@ def mri_case(shape, n_coils: int = 8, accel: float = 6.0, calib: int = 24, noise
     return MRICase(x, S, m, ku.to(torch.complex64), zf.to(torch.complex64))
 
 
-def seed_indices(image: torch.Tensor, num_points: int, seed: int, mode: str = "random") -> torch.Tensor:
+def seed_indices(image: torch.Tensor, num_points: int, seed: int, mode: str = "random",
+                 device=None) -> torch.Tensor:
     """Seed voxels (flat indices, CPU) of the intensity-seeded init, as
     GaussianModel3D.from_image draws them (gaussian_model.py:320-335):
     "random" -- a random permutation of all voxels; "importance" -- a random
     permutation of the voxels whose magnitude exceeds the 90th percentile
-    (all voxels when there are fewer of those than seeds)."""
+    (all voxels when there are fewer of those than seeds).  The permutation
+    always comes from a CPU generator seeded with `seed`; `device` (CUDA)
+    only moves the percentile and the candidate search there, which gives
+    the same candidates (a sort-based quantile either way) in a fraction of
+    the CPU's time."""
     total = image.numel()
     g = torch.Generator().manual_seed(seed)
     n = min(num_points, total)
@@ -265,9 +270,10 @@ def seed_indices(image: torch.Tensor, num_points: int, seed: int, mode: str = "r
         return torch.randperm(total, generator=g)[:n]
     if mode != "importance":
         raise ValueError(f"unknown seeding mode {mode!r}")
-    mag = image.detach().abs().reshape(-1).float().cpu()
+    dev = torch.device(device) if device is not None else torch.device("cpu")
+    mag = image.detach().to(dev).abs().reshape(-1).float()
     thr = torch.quantile(mag, 0.90)
-    cand = torch.nonzero(mag > thr, as_tuple=False).squeeze(-1)
+    cand = torch.nonzero(mag > thr, as_tuple=False).squeeze(-1).cpu()
     if cand.numel() < n:
         cand = torch.arange(total)
     return cand[torch.randperm(cand.numel(), generator=g)[:n]]
@@ -326,7 +332,7 @@ def _from_image_init_gpu(image, num_points, density_scale_k, seed, dev, mode="ra
 
     d, h, w = image.shape
     total = d * h * w
-    idx_cpu = seed_indices(image, num_points, seed, mode)
+    idx_cpu = seed_indices(image, num_points, seed, mode, device=dev)
     n = idx_cpu.numel()
     z = idx_cpu // (h * w)
     rem = idx_cpu % (h * w)

@@ -23,3 +23,14 @@ def test_gpu_knn_init_matches_cktree(shape, n, cuda_device):
     assert torch.equal(gpu.positions.cpu(), cpu.positions)
     assert torch.equal(gpu.density_r.cpu(), cpu.density_r) and torch.equal(gpu.density_i.cpu(), cpu.density_i)
     assert torch.equal(gpu.scales.cpu(), cpu.scales)
+
+
+def test_importance_seeds_are_the_same_on_the_device(cuda_device):
+    """The reference's importance seeding (voxels above the 90th magnitude
+    percentile) gives the same seeds whether the percentile and the
+    candidate search run on the host or on the device."""
+    case = synthetic.mri_case((48, 40, 36), n_coils=4, accel=4.0, calib=12, seed=11)
+    for n in (500, 6000, 10 ** 6):  # the last exceeds the candidates: every voxel is a candidate
+        a = synthetic.seed_indices(case.zero_filled, n, 3, "importance")
+        b = synthetic.seed_indices(case.zero_filled, n, 3, "importance", device=cuda_device)
+        assert torch.equal(a, b)
