@@ -231,6 +231,18 @@ class WarmConfig:
     # (its other mode: voxels above the 90th magnitude percentile); the plain fits that make
     # the targets always seed as the paper profile does
     seed_mode: str = "importance"
+    # learning-rate factor of the fit that starts from the warm start (every parameter group):
+    # the warm start sits close to a good fit, and the plain method's step sizes kick it away
+    fit_lr_scale: float = 0.5
+
+    def fit_overrides(self) -> dict:
+        """FitConfig fields the warm-started fit overrides (the plain method's schedule otherwise)."""
+        if self.fit_lr_scale == 1.0:
+            return {}
+        base = sense.FitConfig()
+        f = self.fit_lr_scale
+        return {"position_lr": base.position_lr * f, "scale_lr": base.scale_lr * f,
+                "rotation_lr": base.rotation_lr * f, "density_lr": base.density_lr * f}
 
 
 @dataclass

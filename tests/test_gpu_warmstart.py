@@ -146,10 +146,12 @@ def _time_to_target_eval(dev, n_train, n_eval, steps, mask_kind="poisson", repor
         case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e, mask_kind=mask_kind)
         rows.append(dict(warmstart.time_to_target(mlp, case, 50_000, seed=e, device=dev,
                                                   warm_points=int(round(50_000 * wc.seed_factor)),
-                                                  warm_mode=wc.seed_mode, ablation=e < ablations), phantom=e))
+                                                  warm_mode=wc.seed_mode, warm_schedule=wc.fit_overrides(),
+                                                  ablation=e < ablations), phantom=e))
     ratios = sorted(r["wall_ratio"] for r in rows if r.get("wall_ratio") is not None)
     report = {"mask": mask_kind, "train_phantoms": n_train, "eval_phantoms": n_eval, "train_steps": steps,
               "seed_factor": wc.seed_factor, "seed_mode": wc.seed_mode, "loss": wc.loss,
+              "fit_lr_scale": wc.fit_lr_scale,
               "train_examples": int(sum(c.features.shape[0] for c in cases)), "data_seconds": t_data,
               "train_seconds": t_train, "first_train_loss": losses[0], "final_train_loss": losses[-1],
               "median_wall_ratio": ratios[len(ratios) // 2] if ratios else None,
