@@ -253,8 +253,8 @@ class TrainingCase:
     base: synthetic.GaussianSet   # intensity-seeded Gaussians (the plain init)
     scale: float
     target: torch.Tensor          # complex64 volume of the plain fit
-    coils: Optional[torch.Tensor] = None  # (C,D,H,W) complex64, for the "dc" loss
-    mask: Optional[torch.Tensor] = None   # (D,H,W) float32, for the "dc" loss
+    coils: Optional[torch.Tensor] = None  # (C,D,H,W) complex64, for the "dc" loss (shared, _shared_coils)
+    mask: Optional[torch.Tensor] = None   # (D,H,W) bool sampling mask, for the "dc" loss
 
 
 def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device, mode: str = "random"):
@@ -270,11 +270,36 @@ def case_inputs(case: synthetic.MRICase, num_points: int, seed: int, device, mod
     return x, vox, base, scale
 
 
-def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
-    """A synthetic phantom, its intensity-seeded Gaussians and the volume the
-    plain method reconstructs from them (the training target)."""
-    case = synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed,
+_COILS = {}
+
+
+def _shared_coils(case: synthetic.MRICase, device) -> torch.Tensor:
+    """One coil-map tensor per (shape, coil count, device) for the "dc" loss
+    of every training case.  The synthetic maps (``synthetic.ring_coils``)
+    of two seeds differ only by a constant phase per coil, and
+    ``_unsampled`` is invariant to it: conj(S e^{ip}) F^-1((1-m) F(S e^{ip} v))
+    = conj(S) F^-1((1-m) F(S v)).  Sharing the first case's maps therefore
+    gives every case its own loss and keeps 57 MB per 96^3 case off the
+    device (``tests/test_warmstart_cpu.py`` checks the invariance)."""
+    key = (tuple(case.sensitivity_maps.shape), str(device))
+    if key not in _COILS:
+        _COILS[key] = case.sensitivity_maps.to(device).to(torch.complex64)
+    return _COILS[key]
+
+
+def synthetic_case(seed: int, wc: WarmConfig) -> synthetic.MRICase:
+    """The seeded training acquisition of ``training_case`` (host-generated)."""
+    return synthetic.mri_case(wc.shape, n_coils=wc.n_coils, accel=wc.accel, calib=wc.calib, seed=seed,
                               mask_kind=wc.mask_kind)
+
+
+def training_case(seed: int, wc: WarmConfig, device="cuda:0",
+                  case: Optional[synthetic.MRICase] = None) -> TrainingCase:
+    """A synthetic phantom, its intensity-seeded Gaussians and the volume the
+    plain method reconstructs from them (the training target).  `case`:
+    ``synthetic_case(seed, wc)`` when the caller made it already."""
+    if case is None:
+        case = synthetic_case(seed, wc)
     n = int(round(wc.points_per_voxel * math.prod(wc.shape)))
     _, _, plain_base, _ = case_inputs(case, n, seed + 1, device)
     if wc.seed_factor == 1.0 and wc.seed_mode == "random":
@@ -293,16 +318,33 @@ def training_case(seed: int, wc: WarmConfig, device="cuda:0") -> TrainingCase:
     with torch.no_grad():
         target = vz(g.positions, g.scales, g.rotations, torch.complex(g.density_r, g.density_i))
     dev = torch.device(device)
-    coils = case.sensitivity_maps.to(dev).to(torch.complex64) if wc.loss == "dc" else None
-    mask = case.mask.to(dev).float() if wc.loss == "dc" else None
+    coils = _shared_coils(case, dev) if wc.loss == "dc" else None
+    mask = (case.mask.to(dev) > 0.5) if wc.loss == "dc" else None
     return TrainingCase(wc.shape, x, vox, base, scale, target.detach(), coils, mask)
+
+
+def training_cases(seeds, wc: WarmConfig, device="cuda:0") -> List[TrainingCase]:
+    """``training_case`` for every seed, with each next acquisition generated
+    on a host thread while the device fits the current one (same cases as
+    one ``training_case`` call per seed)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    seeds = list(seeds)
+    out = []
+    with ThreadPoolExecutor(max_workers=1) as pool:
+        nxt = pool.submit(synthetic_case, seeds[0], wc) if seeds else None
+        for i, s in enumerate(seeds):
+            case = nxt.result()
+            nxt = pool.submit(synthetic_case, seeds[i + 1], wc) if i + 1 < len(seeds) else None
+            out.append(training_case(s, wc, device, case=case))
+    return out
 
 
 def _unsampled(vol: torch.Tensor, coils: torch.Tensor, mask: torch.Tensor) -> torch.Tensor:
     """The part of `vol` hard data consistency leaves in place: the coil
     images' k-space outside the sampling mask, combined back with the coils
     (the difference of two hard-DC volumes is this map of their difference)."""
-    k = synthetic.fft3c(coils * vol.unsqueeze(0)) * (1.0 - mask).unsqueeze(0)
+    k = synthetic.fft3c(coils * vol.unsqueeze(0)) * (~mask if mask.dtype == torch.bool else 1.0 - mask).unsqueeze(0)
     return (torch.conj(coils) * synthetic.ifft3c(k)).sum(0)
 
 

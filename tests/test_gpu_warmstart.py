@@ -133,13 +133,16 @@ def _time_to_target_eval(dev, n_train, n_eval, steps, mask_kind="poisson", repor
     network."""
     wc = warmstart.WarmConfig(mask_kind=mask_kind)
     t0 = time.perf_counter()
-    cases = [warmstart.training_case(1000 + 17 * s, wc, device=dev) for s in range(n_train)]
+    cases = warmstart.training_cases([1000 + 17 * s for s in range(n_train)], wc, device=dev)
     t_data = time.perf_counter() - t0
+    n_examples = int(sum(c.features.shape[0] for c in cases))
     mlp = warmstart.WarmStartMLP(dev, seed=0)
     t0 = time.perf_counter()
     losses = warmstart.train(mlp, cases, steps=steps)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
+    del cases
+    torch.cuda.empty_cache()
     shape = (128, 128, 96)
     rows = []
     for e in range(n_eval):
@@ -152,7 +155,7 @@ def _time_to_target_eval(dev, n_train, n_eval, steps, mask_kind="poisson", repor
     report = {"mask": mask_kind, "train_phantoms": n_train, "eval_phantoms": n_eval, "train_steps": steps,
               "seed_factor": wc.seed_factor, "seed_mode": wc.seed_mode, "loss": wc.loss,
               "fit_lr_scale": wc.fit_lr_scale,
-              "train_examples": int(sum(c.features.shape[0] for c in cases)), "data_seconds": t_data,
+              "train_examples": n_examples, "data_seconds": t_data,
               "train_seconds": t_train, "first_train_loss": losses[0], "final_train_loss": losses[-1],
               "median_wall_ratio": ratios[len(ratios) // 2] if ratios else None,
               "reached": sum(r.get("warm_iterations_to_target") is not None for r in rows),
