@@ -107,6 +107,8 @@ SIGNATURES = {
     "gsv_mlp_gemm": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_longlong, _vp, ctypes.c_longlong,
                                     ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                     _vp, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int, _vp, _vp, _vp]),
+    "gsv_mlp_gemm_test_timeout": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                 ctypes.c_longlong, _vp, _vp]),
     "gsv_sense_workspace_bytes": (_sz, []),
     "gsv_sense_expand": (ctypes.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "gsv_sense_residual": (ctypes.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _sz, _vp]),

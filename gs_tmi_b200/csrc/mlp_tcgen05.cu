@@ -22,7 +22,10 @@
 // shared memory so that stores are coalesced; the GELU' epilogue can also
 // accumulate the column sums of its output (the layer's bias gradient).
 // Every mbarrier wait is bounded; on time-out the kernel latches an error
-// flag, skips the epilogue, frees its TMEM and returns.
+// flag, skips the epilogue, waits (bounded) until the tensor-core work it
+// issued has retired, frees its TMEM and returns.  gsv_mlp_gemm_test_timeout
+// drives that path: thread 0 leaves one K stage's MMAs and commit out, so the
+// wait on that stage runs out.
 // No cluster launch, no multicast, no TMA.
 #include <cuda_bf16.h>
 
@@ -60,6 +63,8 @@ struct GemmArgs {
     int a_mode, b_mode;    // Stage: how each operand is copied to shared memory
     float* col_sum;        // EPI_GELU_GRAD: += column sums of the BF16 output (or null)
     int* error;
+    long long wait_limit;  // polls per mbarrier wait (kWaitLimit unless testing the time-out)
+    int skip_stage;        // test hook: K stage whose MMAs and commit thread 0 leaves out (-1: none)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -89,8 +94,8 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (long long i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -262,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
     constexpr uint32_t kTmemCols = BN < 32 ? 32 : BN;
     static_assert(kStage * STAGES >= kThreads * 33 * 4, "epilogue scratch must fit in the stages");
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bars[STAGES];
+    __shared__ __align__(8) uint64_t bars[STAGES + 1];  // one per stage + the drain barrier of the error path
     __shared__ uint32_t tmem_base_holder;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -282,7 +287,7 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
     }
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
+        for (int s = 0; s <= STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
         cp_async_wait<STAGES - 2>();  // this thread's copies of stage kt have landed
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();              // ... and everyone else's
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && kt != g.skip_stage) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t a_base = smem_u32(smem + (kt % STAGES) * kStage), b_base = a_base + kATile;
 #pragma unroll
@@ -319,7 +324,8 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
         }
         const int nk = kt + STAGES - 1;  // refill the buffer of stage kt - 1 once its MMAs are done
         if (nk < kt_n) {
-            if (kt >= 1) ok = mbar_wait(smem_u32(&bars[(kt - 1) % STAGES]), uint32_t(((kt - 1) / STAGES) & 1));
+            if (kt >= 1)
+                ok = mbar_wait(smem_u32(&bars[(kt - 1) % STAGES]), uint32_t(((kt - 1) / STAGES) & 1), g.wait_limit);
             if (!__syncthreads_and(ok)) break;
             issue(nk);
         }
@@ -327,10 +333,18 @@ __global__ void __launch_bounds__(kThreads, (STAGES <= 2) ? 2 : 1) k_gemm_tcgen0
     }
     cp_async_wait<0>();
     if (ok && kt_n > 0)
-        ok = mbar_wait(smem_u32(&bars[(kt_n - 1) % STAGES]), uint32_t(((kt_n - 1) / STAGES) & 1));
+        ok = mbar_wait(smem_u32(&bars[(kt_n - 1) % STAGES]), uint32_t(((kt_n - 1) / STAGES) & 1), g.wait_limit);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     ok = __syncthreads_and(ok);  // also: every MMA is done with the stages, which become scratch
-    if (!ok && threadIdx.x == 0) atomicOr(g.error, 1);
+    if (!ok && threadIdx.x == 0) {
+        atomicOr(g.error, 1);
+        // A wait ran out, so MMAs committed earlier may not have been waited
+        // for: one more commit arrives on the drain barrier once every
+        // tcgen05 operation this thread issued has completed; TMEM is freed
+        // only after that (or after the bounded wait on it gives up).
+        mma_commit(smem_u32(&bars[STAGES]));
+        mbar_wait(smem_u32(&bars[STAGES]), 0u, kWaitLimit);
+    }
 
     // Epilogue: warp w reads TMEM lanes 32*(w%4).. (the rows it may access)
     // for the columns of group w/4.
@@ -443,14 +457,10 @@ int stage_mode(const void* p, long long s_r, long long s_k) {
     return ST_SCALAR;
 }
 
-}  // namespace
-
-extern "C" {
-
-int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, long long b_sn,
-                         long long b_sk, int M, int N, int K, int splits, const float* bias, float* out_f32,
-                         void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, float* col_sum,
-                         int* error, void* stream) {
+int mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, long long b_sn, long long b_sk, int M,
+             int N, int K, int splits, const float* bias, float* out_f32, void* out_bf16, float* z_f32,
+             long long c_sm, long long c_sn, int epi, float* col_sum, int* error, void* stream,
+             long long wait_limit, int skip_stage) {
     if (!a || !b || !error || M <= 0 || N <= 0 || K <= 0 || (N % 16) != 0 || splits <= 0) return GSV_ERR_INVALID_ARGUMENT;
     if (epi < EPI_F32 || epi > EPI_ATOMIC_F32) return GSV_ERR_INVALID_ARGUMENT;
     if (splits > 1 && epi != EPI_ATOMIC_F32) return GSV_ERR_INVALID_ARGUMENT;
@@ -468,6 +478,7 @@ int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, l
     const int zs = (K + g.k_per_split - 1) / g.k_per_split;
     g.bias = bias; g.out_f32 = out_f32; g.out_bf16 = static_cast<__nv_bfloat16*>(out_bf16); g.z_f32 = z_f32;
     g.c_sm = c_sm; g.c_sn = c_sn; g.epi = epi; g.col_sum = col_sum; g.error = error;
+    g.wait_limit = wait_limit; g.skip_stage = skip_stage;
     g.a_mode = stage_mode(a, a_sm, a_sk);
     g.b_mode = stage_mode(b, b_sn, b_sk);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -481,6 +492,26 @@ int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, l
         default: rc = launch_gemm<EPI_ATOMIC_F32>(g, bn, grid, st); break;
     }
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const void* b, long long b_sn,
+                         long long b_sk, int M, int N, int K, int splits, const float* bias, float* out_f32,
+                         void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, float* col_sum,
+                         int* error, void* stream) {
+    return mlp_gemm(a, a_sm, a_sk, b, b_sn, b_sk, M, N, K, splits, bias, out_f32, out_bf16, z_f32, c_sm, c_sn, epi,
+                    col_sum, error, stream, kWaitLimit, -1);
+}
+
+int gsv_mlp_gemm_test_timeout(const void* a, const void* b, int M, int N, int K, float* out_f32, int skip_stage,
+                              long long wait_limit, int* error, void* stream) {
+    if (skip_stage < 0 || skip_stage >= (K + kBK - 1) / kBK) return GSV_ERR_INVALID_ARGUMENT;
+    if (wait_limit <= 0 || wait_limit > kWaitLimit) return GSV_ERR_INVALID_ARGUMENT;
+    return mlp_gemm(a, K, 1, b, K, 1, M, N, K, 1, nullptr, out_f32, nullptr, nullptr, N, 1, EPI_F32, nullptr, error,
+                    stream, wait_limit, skip_stage);
 }
 
 }  // extern "C"

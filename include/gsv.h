@@ -282,6 +282,16 @@ GSV_API int gsv_mlp_gemm(const void* a, long long a_sm, long long a_sk, const vo
                          void* out_bf16, float* z_f32, long long c_sm, long long c_sn, int epi, float* col_sum,
                          int* error, void* stream);
 
+/* Test hook for the time-out path of gsv_mlp_gemm: C = A B^T (A [M,K], B [N,K]
+ * row-major BF16, C [M,N] FP32) with the tensor-core work of K stage
+ * `skip_stage` (64 columns of K each, 0 <= skip_stage < ceil(K/64)) left out,
+ * so that the wait on it runs out after `wait_limit` polls (1 .. 2^26).  Every
+ * CTA then sets *error = 1, waits for the tensor-core work it did issue,
+ * frees its tensor memory and returns without writing C; the stream stays
+ * usable.  Not for computing anything. */
+GSV_API int gsv_mlp_gemm_test_timeout(const void* a, const void* b, int M, int N, int K, float* out_f32,
+                                      int skip_stage, long long wait_limit, int* error, void* stream);
+
 /* ---- fused SENSE data term around the FFTs ---------------------------- */
 
 /* Replace the elementwise torch ops of the plain loss's data term

@@ -90,3 +90,31 @@ def test_gemm_gelu_epilogues(cuda_device):
     assert rel(dz.float(), zz.grad) < 1e-2
     # fused bias gradient: column sums of the stored BF16 output
     assert rel(colsum, dz.float().sum(0)) < 1e-5
+
+
+def test_tensor_core_wait_time_out_is_reported(cuda_device):
+    """The bounded mbarrier wait's error path: with one K stage's MMAs and
+    commit left out (first, middle and last of four stages) the wait on that
+    stage runs out after 1024 polls; every CTA latches the error flag and
+    returns without its epilogue (C keeps its NaN fill), and the stream and
+    the regular GEMM still work afterwards."""
+    M, N, K = 256, 256, 256
+    g = torch.Generator(device=cuda_device).manual_seed(11)
+    a = torch.randn(M, K, device=cuda_device, generator=g).bfloat16()
+    b = torch.randn(N, K, device=cuda_device, generator=g).bfloat16()
+    err = torch.zeros(1, dtype=torch.int32, device=cuda_device)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for skip in (0, 1, 3):
+        out = torch.full((M, N), float("nan"), device=cuda_device)
+        err.zero_()
+        check(lib.gsv_mlp_gemm_test_timeout(_p(a), _p(b), M, N, K, _p(out), skip, 1 << 10, _p(err), st),
+              "gsv_mlp_gemm_test_timeout")
+        torch.cuda.synchronize()
+        assert int(err.item()) == 1, skip
+        assert bool(torch.isnan(out).all()), skip
+    # out-of-range hooks are refused before any launch
+    for skip, limit in ((4, 1024), (-1, 1024), (0, 0), (0, (1 << 26) + 1)):
+        assert lib.gsv_mlp_gemm_test_timeout(_p(a), _p(b), M, N, K, _p(out), skip, limit, _p(err), st) != 0
+    out = torch.empty(M, N, device=cuda_device)
+    gemm(a, (K, 1), b, (K, 1), M, N, K, EPI_F32, out_f32=out)
+    assert rel(out, a.float() @ b.float().t()) < 1e-5
