@@ -26,6 +26,8 @@ GSV_FLAG_SCAN_STALLED = 0x8
 GSV_BACKWARD_DETERMINISTIC = 0x1
 GSV_TUNE_NO_CULL = 0x1
 
+GSV_BIN_AUTO, GSV_BIN_RADIX, GSV_BIN_COUNTING = 0, 1, 2
+
 
 class GsvShape(ctypes.Structure):
     _fields_ = [("d", ctypes.c_int32), ("h", ctypes.c_int32), ("w", ctypes.c_int32),
@@ -89,6 +91,7 @@ SIGNATURES = {
     "gsv_prepare": (ctypes.c_int, [_P, _S, _vp, _sz, _i64p, _vp]),
     "gsv_prepare_live": (ctypes.c_int, [_P, _vp, _S, _vp, _sz, _i64p, _vp]),
     "gsv_bin": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, _vp]),
+    "gsv_bin_ex": (ctypes.c_int, [_S, _i64, _vp, _vp, _sz, _i64, ctypes.c_int, _vp]),
     "gsv_bin_views": (ctypes.c_int, [_S, _i64, _vp, _vp, _i64, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsv_status_views": (ctypes.c_int, [_S, _i64, _vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "gsv_read_status": (ctypes.c_int, [_S, _i64, _vp, _i64p, _i32p, _vp]),

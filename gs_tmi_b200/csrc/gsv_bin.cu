@@ -58,8 +58,35 @@ int sort_end_bit(int64_t ntiles) {
 // region that starts every preprocess.
 constexpr int kPrepThreads = 256;
 __host__ __device__ inline int64_t prep_blocks(int64_t n) { return (n + 1 + kPrepThreads - 1) / kPrepThreads; }
-__host__ __device__ inline size_t status_bytes(int64_t n) {
-    return sizeof(Status) + size_t(prep_blocks(n)) * sizeof(unsigned long long);
+
+// Counting-sort binning, used when the tile count is small.  The pairs'
+// final order is fixed by two facts: a tile's list holds its Gaussians in
+// ascending id, and Gaussians are handled in rows of kCsSeg consecutive ids.
+// k_prepare also writes, per row, how many of the row's pairs fall in each
+// tile (rows x tiles int32, "cs_mat"); k_colscan writes, per row and tile,
+// the position of the row's first pair of that tile in the sorted output
+// ("cs_pos": the column's exclusive prefix plus the tile's start, from a
+// single-pass scan of the tile totals) and the tile ranges; k_scatter walks
+// each row's Gaussians in id order and places their pairs.  The result
+// equals the stable radix sort's, which larger problems keep.  The counts
+// stay intact and k_scatter clears k_colscan's scan state, so binning may
+// be repeated after one preprocess (e.g. with a larger capacity).
+constexpr int kCsSeg = 64;                                  // Gaussians per row: two warps of k_prepare
+constexpr int kCsRowsPerBlock = kPrepThreads / kCsSeg;      // rows per k_prepare block
+constexpr int64_t kCsMaxTiles = 4096;                       // k_prepare / k_scatter keep rows x tiles in smem
+constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles int32: 16 MB per matrix
+constexpr int kCsCols = 32, kCsRowGroups = 32;              // k_colscan block: 32 columns x 32 row groups
+__host__ __device__ inline int64_t cs_rows(int64_t n) { return prep_blocks(n) * kCsRowsPerBlock; }
+__host__ __device__ inline int64_t cs_col_blocks(int64_t ntiles) { return (ntiles + kCsCols - 1) / kCsCols; }
+inline bool cs_eligible(int64_t n, int64_t ntiles) {
+    return n > 0 && ntiles <= kCsMaxTiles && cs_rows(n) * ntiles <= kCsMaxCells;
+}
+
+// Status region: the Status word, the preprocess's look-back words (one per
+// block), then k_colscan's (one per column block).  Status::pad[1] and
+// pad[2] are the two launches' block-ticket counters.
+__host__ __device__ inline size_t status_bytes(int64_t n, int64_t ntiles) {
+    return sizeof(Status) + size_t(prep_blocks(n) + cs_col_blocks(ntiles)) * sizeof(unsigned long long);
 }
 
 GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
@@ -77,7 +104,10 @@ GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
     L.scan_tmp = o; o = align_up(o + scan_bytes);
     L.ranges = o;   o = align_up(o + size_t(si.ntiles) * sizeof(int2));
     L.accum = o;    o = align_up(o + size_t(n) * kMomStride * sizeof(float));
-    L.status = o;   o = align_up(o + status_bytes(n));
+    L.status = o;   o = align_up(o + status_bytes(n, si.ntiles));
+    L.cs = cs_eligible(n, si.ntiles);
+    L.cs_mat = o;   o = align_up(o + (L.cs ? size_t(cs_rows(n) * si.ntiles) * sizeof(int32_t) : 0));
+    L.cs_pos = o;   o = align_up(o + (L.cs ? size_t(cs_rows(n) * si.ntiles) * sizeof(int32_t) : 0));
     L.total = o;
     return L;
 }
@@ -179,6 +209,63 @@ __device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long lo
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// Decoupled look-back of scan block `bid`, run by all 32 lanes of one warp:
+// publishes the block's total, walks back over the predecessors' words and
+// returns the sum of every earlier block's total (the same in all lanes),
+// after publishing its own inclusive prefix.  Lane l reads the word of block
+// j - l, so one step covers 32 predecessors; the nearest inclusive prefix
+// (kLbPre) in the window ends the walk, and every word in front of it must
+// be published (flag set) before the window is summed, else the step is
+// retried.  Block ids come from a ticket counter, so every block waited for
+// has started.  Each retry is bounded: on time-out GSV_FLAG_SCAN_STALLED is
+// latched and the block publishes what it has, so no later block waits the
+// full limit again.
+__device__ int64_t lookback(unsigned long long* lb, int64_t bid, int64_t block_tot, Status* status, int lane) {
+    if (bid == 0) {
+        if (lane == 0) lb_store(&lb[0], kLbPre | (unsigned long long)block_tot);
+        return 0;
+    }
+    if (lane == 0) lb_store(&lb[bid], kLbAgg | (unsigned long long)block_tot);
+    int64_t base = 0;
+    int64_t j = bid - 1;  // the window's nearest predecessor
+    int spins = 0;
+    while (true) {
+        const int64_t idx = j - lane;
+        // before block 0 there is nothing: an inclusive prefix of zero
+        const unsigned long long v = idx >= 0 ? lb_load(&lb[idx]) : kLbPre;
+        const unsigned long long f = v & ~kLbVal;
+        const unsigned pre = __ballot_sync(0xffffffffu, f == kLbPre);
+        const int first = pre ? __ffs(pre) - 1 : 31;  // last lane of this step
+        const unsigned upto = first == 31 ? 0xffffffffu : (2u << first) - 1u;
+        const unsigned missing = __ballot_sync(0xffffffffu, f == 0) & upto;
+        if (missing) {
+            if (++spins > kLbSpinLimit) {
+                if (lane == 0) atomicOr(&status->flags, GSV_FLAG_SCAN_STALLED);
+                break;
+            }
+            continue;
+        }
+        spins = 0;
+        int64_t part = ((upto >> lane) & 1u) ? int64_t(v & kLbVal) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        base += part;
+        if (pre) break;
+        j -= 32;
+    }
+    if (lane == 0) lb_store(&lb[bid], kLbPre | (unsigned long long)(base + block_tot));
+    return base;
+}
+
+// Tile id of pair `c` (0-based, raster order) of a Gaussian's packed tile box.
+__device__ __forceinline__ int32_t box_tile(const DevShape& s, int bx, int by, int bz, int32_t c) {
+    const int32_t t0 = bx & 0xffff, t1 = (bx >> 16) & 0xffff, t2 = by & 0xffff;
+    const int32_t n1 = bz & 0xffff, n2 = (bz >> 16) & 0xffff;
+    const int32_t k = c % n2, r = c / n2;
+    const int32_t jj = r % n1, i = r / n1;
+    return ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
+}
+
 // Preprocess (center, radius, quadratic-form coefficients, tight extent, tile
 // box) of one Gaussian per thread, and the exclusive scan of the Gaussians'
 // pair counts into `offsets` (offsets[n] = pair total) in the same launch.
@@ -186,7 +273,10 @@ __device__ __forceinline__ void lb_store(unsigned long long* p, unsigned long lo
 // region, so every block a block waits for has already started; it waits
 // only for its predecessors' published totals, each wait bounded (on
 // time-out GSV_FLAG_SCAN_STALLED is latched and the block publishes anyway,
-// so no later block waits the full limit again).
+// so no later block waits the full limit again).  With `cs_mat` the block
+// also counts its pairs per tile for each of its kCsRowsPerBlock rows
+// (dynamic shared memory: kCsRowsPerBlock x ntiles int32) and writes those
+// rows of cs_mat.
 __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restrict__ pos,
                                                           const float* __restrict__ scl,
                                                           const float* __restrict__ rot,
@@ -195,7 +285,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
                                                           const int32_t* __restrict__ live, DevShape s,
                                                           Rec* __restrict__ recs, float4* __restrict__ ext,
                                                           int4* __restrict__ boxes,
-                                                          int64_t* __restrict__ offsets, Status* status) {
+                                                          int64_t* __restrict__ offsets, Status* status,
+                                                          int32_t* __restrict__ cs_mat, int32_t ntiles) {
     __shared__ int bid_s;
     __shared__ int64_t warp_tot[kPrepThreads / 32];
     __shared__ int64_t block_base;
@@ -204,6 +295,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
     const int64_t bid = bid_s;
     const int64_t g = bid * kPrepThreads + threadIdx.x;
     int64_t cnt = 0;
+    int4 box = make_int4(0, 0, 0, 0);
     if (g < n && live && g >= int64_t(*live)) {  // parked row: no tiles, no contribution
         recs[g] = Rec{};
         ext[g] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -233,7 +325,6 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
         R.rho_r = dr[g]; R.rho_i = di[g]; R.pad = 0.0f;
         recs[g] = R;
         ext[g] = tight_extent(qc);
-        int4 box;
         cnt = tile_box(s, c, r, &box);
         if (cnt <= 0) {
             atomicOr(&status->flags, GSV_FLAG_EMPTY_BOX);
@@ -259,48 +350,44 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
         block_tot += warp_tot[w];
     }
     if (warp == 0) {
-        // Look-back by the whole first warp: lane l reads the word of block j - l, so one
-        // step covers 32 predecessors.  The nearest inclusive prefix (kLbPre) in the window
-        // ends the walk; every word in front of it must be published (flag set) before the
-        // window is summed, else the step is retried (bounded).
-        unsigned long long* lb = reinterpret_cast<unsigned long long*>(status + 1);
-        int64_t base = 0;
-        if (bid == 0) {
-            if (lane == 0) lb_store(&lb[0], kLbPre | (unsigned long long)block_tot);
-        } else {
-            if (lane == 0) lb_store(&lb[bid], kLbAgg | (unsigned long long)block_tot);
-            int64_t j = bid - 1;  // the window's nearest predecessor
-            int spins = 0;
-            while (true) {
-                const int64_t idx = j - lane;
-                // before block 0 there is nothing: an inclusive prefix of zero
-                const unsigned long long v = idx >= 0 ? lb_load(&lb[idx]) : kLbPre;
-                const unsigned long long f = v & ~kLbVal;
-                const unsigned pre = __ballot_sync(0xffffffffu, f == kLbPre);
-                const int first = pre ? __ffs(pre) - 1 : 31;        // last lane of this step
-                const unsigned upto = first == 31 ? 0xffffffffu : (2u << first) - 1u;
-                const unsigned missing = __ballot_sync(0xffffffffu, f == 0) & upto;
-                if (missing) {
-                    if (++spins > kLbSpinLimit) {
-                        if (lane == 0) atomicOr(&status->flags, GSV_FLAG_SCAN_STALLED);
-                        break;
-                    }
-                    continue;
-                }
-                spins = 0;
-                int64_t part = ((upto >> lane) & 1u) ? int64_t(v & kLbVal) : 0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-                base += part;
-                if (pre) break;
-                j -= 32;
-            }
-            if (lane == 0) lb_store(&lb[bid], kLbPre | (unsigned long long)(base + block_tot));
-        }
+        const int64_t base = lookback(reinterpret_cast<unsigned long long*>(status + 1), bid, block_tot, status, lane);
         if (lane == 0) block_base = base;
     }
     __syncthreads();
     if (g <= n) offsets[g] = block_base + warp_base + incl - cnt;
+    if (cs_mat == nullptr) return;  // block-uniform
+
+    // Per-row tile counts.  The warp's pairs occupy the block-local range
+    // [wstart, wend), lane l's Gaussian the part starting at o; the lanes
+    // stride over the range and find each pair's Gaussian by a shuffle
+    // search over the 32 starts (zero-count lanes share their successor's
+    // start and are never chosen).
+    extern __shared__ int32_t cs_hist[];  // [kCsRowsPerBlock][ntiles]
+    for (int i = threadIdx.x; i < kCsRowsPerBlock * ntiles; i += kPrepThreads) cs_hist[i] = 0;
+    __syncthreads();
+    {
+        constexpr unsigned kAll = 0xffffffffu;
+        const long long o = warp_base + incl - cnt;
+        const long long wstart = __shfl_sync(kAll, o, 0);
+        const long long wend = warp_base + warp_tot[warp];
+        int32_t* row = cs_hist + (warp * 32 / kCsSeg) * ntiles;
+        for (long long base = wstart; base < wend; base += 32) {
+            const long long p = base + lane;
+            int j = 0;  // largest j with o_j <= p
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const long long oj = __shfl_sync(kAll, o, j + step);
+                if (oj <= p) j += step;
+            }
+            const long long oj = __shfl_sync(kAll, o, j);
+            const int bx = __shfl_sync(kAll, box.x, j), by = __shfl_sync(kAll, box.y, j),
+                      bz = __shfl_sync(kAll, box.z, j);
+            if (p < wend) atomicAdd(&row[box_tile(s, bx, by, bz, int32_t(p - oj))], 1);
+        }
+    }
+    __syncthreads();
+    int32_t* dst = cs_mat + bid * kCsRowsPerBlock * int64_t(ntiles);
+    for (int i = threadIdx.x; i < kCsRowsPerBlock * ntiles; i += kPrepThreads) dst[i] = cs_hist[i];
 }
 
 __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ center,
@@ -399,6 +486,121 @@ __global__ void k_ranges(const int32_t* __restrict__ keys, const int64_t* __rest
     if (i == total - 1 || keys[i + 1] != key) ranges[key].y = int32_t(i + 1);
 }
 
+// Column pass of the counting sort: one block per kCsCols tiles (dynamic
+// block id from Status::pad[2]), 32 row groups per column.  cs_pos[r][t] =
+// start(t) + the pairs of rows < r in tile t, where start(t) = the pairs in
+// tiles < t, from a single-pass look-back over the blocks' tile totals.
+// Writes every tile's range, (0,0) for an empty tile, clamped to `cap` (so a
+// truncated list never reaches past the pair buffer).
+__global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const int32_t* __restrict__ mat,
+                                                                    int32_t* __restrict__ pos, int64_t rows,
+                                                                    int32_t ntiles, int64_t cap,
+                                                                    int2* __restrict__ ranges, Status* status,
+                                                                    unsigned long long* lb) {
+    __shared__ int bid_s;
+    __shared__ int64_t part[kCsRowGroups][kCsCols];  // a row group's sum, then its exclusive prefix
+    __shared__ int64_t start_s[kCsCols], tot_s[kCsCols];
+    if (threadIdx.x == 0) bid_s = atomicAdd(&status->pad[2], 1);
+    __syncthreads();
+    const int64_t bid = bid_s;
+    const int c = threadIdx.x % kCsCols, rg = threadIdx.x / kCsCols;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t t = bid * kCsCols + c;
+    const bool col_ok = t < ntiles;
+    const int64_t per = (rows + kCsRowGroups - 1) / kCsRowGroups;
+    const int64_t r0 = min(rows, rg * per), r1 = min(rows, r0 + per);
+    int64_t sum = 0;
+    if (col_ok) {
+#pragma unroll 8
+        for (int64_t r = r0; r < r1; ++r) sum += mat[r * ntiles + t];
+    }
+    part[rg][c] = sum;
+    __syncthreads();
+    if (warp == 0) {  // lane = column of this block
+        int64_t run = 0;
+        for (int k = 0; k < kCsRowGroups; ++k) {
+            const int64_t v = part[k][lane];
+            part[k][lane] = run;
+            run += v;
+        }
+        tot_s[lane] = run;
+        int64_t incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int64_t block_tot = __shfl_sync(0xffffffffu, incl, 31);
+        const int64_t base = lookback(lb, bid, block_tot, status, lane);
+        start_s[lane] = base + incl - run;
+    }
+    __syncthreads();
+    if (!col_ok) return;
+    int64_t at_r = start_s[c] + part[rg][c];
+    for (int64_t r = r0; r < r1; ++r) {
+        const int64_t idx = r * ntiles + t;
+        pos[idx] = int32_t(min(at_r, cap));
+        at_r += mat[idx];
+    }
+    if (rg == 0) {
+        const int64_t st = start_s[c], tt = tot_s[c];
+        ranges[t] = tt > 0 ? make_int2(int32_t(min(st, cap)), int32_t(min(st + tt, cap))) : make_int2(0, 0);
+    }
+}
+
+// Placement pass of the counting sort: one warp per row of kCsSeg
+// Gaussians, kCsRowsPerBlock rows per block.  The warp copies its row of
+// positions to shared memory, then walks the row's Gaussians in ascending
+// id: the lanes take the Gaussian's tiles (distinct tiles, so no two lanes
+// share a counter), write its id at each tile's current position and advance
+// it.  Positions at or past `cap` are dropped (the overflow flag says so).
+// Block 0 also latches the capacity flags and clears k_colscan's ticket
+// counter and look-back words (k_colscan has finished: stream order).
+__global__ void __launch_bounds__(32 * kCsRowsPerBlock) k_scatter(const int32_t* __restrict__ pos_in,
+                                                                  const int4* __restrict__ boxes,
+                                                                  const int64_t* __restrict__ offsets, int64_t n,
+                                                                  int32_t ntiles, int64_t rows, DevShape s,
+                                                                  int64_t cap, int32_t* __restrict__ pair_ids,
+                                                                  Status* status, unsigned long long* lb,
+                                                                  int64_t lb_words) {
+    constexpr unsigned kAll = 0xffffffffu;
+    extern __shared__ int32_t cs_at[];  // [kCsRowsPerBlock][ntiles]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            const int64_t total = offsets[n];
+            if (total > cap) atomicOr(&status->flags, GSV_FLAG_CAPACITY_OVERFLOW);
+            if (total > int64_t(INT32_MAX)) atomicOr(&status->flags, GSV_FLAG_TOO_MANY_PAIRS);
+            status->pad[2] = 0;
+        }
+        for (int64_t i = threadIdx.x; i < lb_words; i += blockDim.x) lb[i] = 0ull;
+    }
+    const int64_t row = int64_t(blockIdx.x) * kCsRowsPerBlock + warp;
+    if (row >= rows) return;  // warp-uniform; no block barrier follows
+    int32_t* at_t = cs_at + warp * ntiles;
+    for (int t = lane; t < ntiles; t += 32) at_t[t] = pos_in[row * ntiles + t];
+    __syncwarp();
+    const int64_t g0 = row * kCsSeg;
+    for (int h = 0; h < kCsSeg; h += 32) {
+        const int64_t gl = g0 + h + lane;
+        const int4 mb = gl < n ? boxes[gl] : make_int4(0, 0, 0, 0);
+        for (int k = 0; k < 32; ++k) {  // the Gaussians in ascending id
+            const int cnt = __shfl_sync(kAll, mb.w, k);
+            const int bx = __shfl_sync(kAll, mb.x, k), by = __shfl_sync(kAll, mb.y, k),
+                      bz = __shfl_sync(kAll, mb.z, k);
+            if (cnt <= 0) continue;  // warp-uniform
+            const int32_t gid = int32_t(g0 + h + k);
+            for (int c = lane; c < cnt; c += 32) {
+                const int32_t t = box_tile(s, bx, by, bz, c);
+                const int32_t p = at_t[t];
+                if (p < cap) pair_ids[p] = gid;
+                at_t[t] = int32_t(min(int64_t(p) + 1, cap));
+            }
+            __syncwarp();
+        }
+    }
+}
+
 int grid_for(int64_t items, int block) {
     int64_t g = (items + block - 1) / block;
     if (g < 1) g = 1;
@@ -415,10 +617,22 @@ int sync_total(const GaussLayout& L, void* ws, int64_t n, int64_t* total_host, c
     return GSV_OK;
 }
 
-// Shared tail of both binning flavours: emit, sort, ranges.
+int cs_smem_bytes(int64_t ntiles) { return int(kCsRowsPerBlock * ntiles * int64_t(sizeof(int32_t))); }
+
+template <typename K>
+int allow_smem(K kernel, int bytes) {
+    if (bytes > 48 * 1024)
+        GSV_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return GSV_OK;
+}
+
+// Shared tail of both binning flavours.  Counting sort (k_colscan,
+// k_scatter) when the preprocess wrote the per-row tile counts (native path,
+// small tile count) and `mode` allows it; otherwise emit, radix sort, ranges.
 int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
-               int64_t cap, int32_t* vals_out_override, cudaStream_t st) {
+               int64_t cap, int32_t* vals_out_override, int mode, bool rows_written, cudaStream_t st) {
     if (cap < 0 || cap > int64_t(INT32_MAX)) return GSV_ERR_INVALID_ARGUMENT;
+    if (mode != GSV_BIN_AUTO && mode != GSV_BIN_RADIX && mode != GSV_BIN_COUNTING) return GSV_ERR_INVALID_ARGUMENT;
     const GaussLayout G = gauss_layout(n, si);
     const PairLayout P = pair_layout(cap, si, 0);
     if (ws_pairs_bytes < P.total || !ws_pairs) return GSV_ERR_INVALID_ARGUMENT;
@@ -430,8 +644,25 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
     int32_t* keys_out = at<int32_t>(ws_pairs, P.keys_out);
     int32_t* vals_out = vals_out_override ? vals_out_override : at<int32_t>(ws_pairs, P.vals_out);
     int2* ranges = at<int2>(ws_gauss, G.ranges);
+    const bool cs = rows_written && G.cs;
+    if (mode == GSV_BIN_COUNTING && !cs) return GSV_ERR_INVALID_ARGUMENT;
     if (cap == 0) {
         GSV_CUDA_TRY(cudaMemsetAsync(ranges, 0, size_t(si.ntiles) * sizeof(int2), st));
+        return GSV_OK;
+    }
+    if (cs && mode != GSV_BIN_RADIX) {
+        unsigned long long* lb_cs = reinterpret_cast<unsigned long long*>(status + 1) + prep_blocks(n);
+        const int64_t rows = cs_rows(n);
+        const int32_t T = int32_t(si.ntiles);
+        k_colscan<<<unsigned(cs_col_blocks(T)), kCsCols * kCsRowGroups, 0, st>>>(
+            at<int32_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
+        GSV_LAUNCH_CHECK();
+        const int smem = cs_smem_bytes(T);
+        if (int rc = allow_smem(k_scatter, smem)) return rc;
+        k_scatter<<<unsigned(prep_blocks(n)), 32 * kCsRowsPerBlock, smem, st>>>(
+            at<int32_t>(ws_gauss, G.cs_pos), at<int4>(ws_gauss, G.box), offsets, n, T, rows, s, cap, vals_out, status,
+            lb_cs, cs_col_blocks(T));
+        GSV_LAUNCH_CHECK();
         return GSV_OK;
     }
     // enough CTAs for the emission (one thread per Gaussian) and for the fills
@@ -507,12 +738,15 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
     if (ws_gauss_bytes < L.total) return GSV_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Status* status = at<Status>(ws_gauss, L.status);
-    // status flags, the block counter and the scan's look-back words
-    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, status_bytes(n), st));
-    k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, 0, st>>>(
+    // status flags, the block counters and the scans' look-back words
+    GSV_CUDA_TRY(cudaMemsetAsync(status, 0, status_bytes(n, si.ntiles), st));
+    const int smem = L.cs ? cs_smem_bytes(si.ntiles) : 0;
+    if (int rc = allow_smem(k_prepare, smem)) return rc;
+    k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, smem, st>>>(
         p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
         at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),
-        at<int64_t>(ws_gauss, L.offsets), status);
+        at<int64_t>(ws_gauss, L.offsets), status, L.cs ? at<int32_t>(ws_gauss, L.cs_mat) : nullptr,
+        int32_t(si.ntiles));
     GSV_LAUNCH_CHECK();
     if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
     return GSV_OK;
@@ -529,12 +763,17 @@ int gsv_prepare_live(const gsv_params* p, const int32_t* live, gsv_shape shape, 
     return prepare_impl(p, live, shape, ws_gauss, ws_gauss_bytes, total_pairs_host, stream);
 }
 
-int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
-            int64_t capacity, void* stream) {
+int gsv_bin_ex(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+               int64_t capacity, int mode, void* stream) {
     ShapeInfo si = shape_info(shape);
     if (!si.ok || n < 0 || !ws_gauss) return GSV_ERR_INVALID_ARGUMENT;
-    return bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, nullptr,
+    return bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, nullptr, mode, true,
                       static_cast<cudaStream_t>(stream));
+}
+
+int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+            int64_t capacity, void* stream) {
+    return gsv_bin_ex(shape, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, GSV_BIN_AUTO, stream);
 }
 
 int gsv_bin_views(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, int64_t capacity,
@@ -603,7 +842,7 @@ int gsv_build_tile_pairs_fill(gsv_shape shape, int64_t n, void* ws_gauss, void* 
     if (!si.ok || n < 0 || !ws_gauss || !tile_ranges || (capacity > 0 && !pair_ids))
         return GSV_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int rc = bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, pair_ids, st);
+    int rc = bin_common(si, n, ws_gauss, ws_pairs, ws_pairs_bytes, capacity, pair_ids, GSV_BIN_RADIX, false, st);
     if (rc != GSV_OK) return rc;
     const GaussLayout L = gauss_layout(n, si);
     GSV_CUDA_TRY(cudaMemcpyAsync(tile_ranges, at<int2>(ws_gauss, L.ranges), size_t(si.ntiles) * sizeof(int2),

@@ -155,8 +155,9 @@ __device__ __forceinline__ float row_m(float q22, float a, float b, float e2) {
 __host__ __device__ inline size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct GaussLayout {
-    size_t rec, ext, box, counts, offsets, scan_tmp, ranges, accum, status, total;
+    size_t rec, ext, box, counts, offsets, scan_tmp, ranges, accum, status, cs_mat, cs_pos, total;
     size_t scan_tmp_bytes;
+    bool cs;  // the counting-sort binning applies (cs_mat: per-row tile counts, cs_pos: positions)
 };
 
 struct PairLayout {

@@ -50,7 +50,7 @@
 extern "C" {
 #endif
 
-#define GSV_ABI_VERSION 3
+#define GSV_ABI_VERSION 4
 
 typedef enum gsv_status {
     GSV_OK = 0,
@@ -127,12 +127,23 @@ GSV_API int gsv_prepare(const gsv_params* params, gsv_shape shape, void* ws_gaus
 GSV_API int gsv_prepare_live(const gsv_params* params, const int32_t* live, gsv_shape shape, void* ws_gauss,
                              size_t ws_gauss_bytes, int64_t* total_pairs_host, void* stream);
 
-/* Emit (tile, Gaussian) pairs, radix-sort them by tile (stable: ascending
- * Gaussian id within a tile) and build the per-tile ranges.  If the pair
- * total exceeds `capacity` only `capacity` pairs are kept and
- * GSV_FLAG_CAPACITY_OVERFLOW is latched. */
+/* Sort the (tile, Gaussian) pairs of the last gsv_prepare / gsv_prepare_live
+ * on this workspace by tile (stable: ascending Gaussian id within a tile)
+ * and build the per-tile ranges.  If the pair total exceeds `capacity` only
+ * `capacity` pairs are kept and GSV_FLAG_CAPACITY_OVERFLOW is latched.  May
+ * be called again after one preprocess (e.g. with a larger capacity).
+ * Two sorts give the same lists: a counting sort over per-row tile counts
+ * the preprocess writes when the grid has at most 4096 tiles and
+ * ceil((n+1)/256)*4 rows x tiles <= 2^22 (three launches, no pair
+ * keys), else an emit + radix sort + range pass.  gsv_bin picks the first
+ * where it applies. */
+#define GSV_BIN_AUTO 0
+#define GSV_BIN_RADIX 1    /* always the radix sort */
+#define GSV_BIN_COUNTING 2 /* the counting sort; GSV_ERR_INVALID_ARGUMENT where it does not apply */
 GSV_API int gsv_bin(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
             int64_t capacity, void* stream);
+GSV_API int gsv_bin_ex(gsv_shape shape, int64_t n, void* ws_gauss, void* ws_pairs, size_t ws_pairs_bytes,
+                       int64_t capacity, int mode, void* stream);
 
 /* Pointers to the tile ranges (int32 [T,2], empty tiles (0,0)) and the
  * sorted pair ids (int32 [capacity]) held inside the workspaces. */

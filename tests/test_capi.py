@@ -44,7 +44,7 @@ def test_library_exports_every_declared_symbol():
 def test_host_queries():
     from gs_tmi_b200._lib import GsvShape, lib
 
-    assert lib.gsv_abi_version() == 3
+    assert lib.gsv_abi_version() == 4
     s = GsvShape(64, 64, 64, 8)
     assert lib.gsv_num_tiles(s) == 512
     assert lib.gsv_num_tiles(GsvShape(20, 12, 16, 8)) == 3 * 2 * 2
@@ -149,15 +149,15 @@ def test_density_host_queries():
 
 
 def test_flag_and_status_constants_mirror_the_header():
-    """Every GSV_FLAG_*, GSV_BACKWARD_* and GSV_TUNE_* #define of
-    include/gsv.h has the same value in the ctypes binding."""
+    """Every GSV_FLAG_*, GSV_BACKWARD_*, GSV_TUNE_*, GSV_DENSITY_* and GSV_BIN_*
+    #define of include/gsv.h has the same value in the ctypes binding."""
     import re
 
     from gs_tmi_b200 import _lib
 
     text = open(os.path.join(ROOT, "include", "gsv.h")).read()
-    defs = dict(re.findall(r"^#define\s+(GSV_(?:FLAG|BACKWARD|TUNE|DENSITY)_\w+)\s+(0x[0-9a-fA-F]+|\d+)", text,
+    defs = dict(re.findall(r"^#define\s+(GSV_(?:FLAG|BACKWARD|TUNE|DENSITY|BIN)_\w+)\s+(0x[0-9a-fA-F]+|\d+)", text,
                            flags=re.M))
-    assert "GSV_FLAG_SCAN_STALLED" in defs
+    assert "GSV_FLAG_SCAN_STALLED" in defs and "GSV_BIN_COUNTING" in defs
     for name, value in defs.items():
         assert getattr(_lib, name) == int(value, 0), name
