@@ -73,7 +73,9 @@ __host__ __device__ inline int64_t prep_blocks(int64_t n) { return (n + 1 + kPre
 // be repeated after one preprocess (e.g. with a larger capacity).
 constexpr int kCsSeg = 64;                                  // Gaussians per row: two warps of k_prepare
 constexpr int kCsRowsPerBlock = kPrepThreads / kCsSeg;      // rows per k_prepare block
-constexpr int64_t kCsMaxTiles = 4096;                       // k_prepare / k_scatter keep rows x tiles in smem
+// k_prepare and k_scatter keep kCsRowsPerBlock x ntiles int32 in shared memory: at most 48 KB, the
+// size a launch may use without a function attribute (none is set, also not inside a graph capture)
+constexpr int64_t kCsMaxTiles = 3072;
 constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles int32: 16 MB per matrix
 constexpr int kCsCols = 32, kCsRowGroups = 32;              // k_colscan block: 32 columns x 32 row groups
 __host__ __device__ inline int64_t cs_rows(int64_t n) { return prep_blocks(n) * kCsRowsPerBlock; }
@@ -618,13 +620,7 @@ int sync_total(const GaussLayout& L, void* ws, int64_t n, int64_t* total_host, c
 }
 
 int cs_smem_bytes(int64_t ntiles) { return int(kCsRowsPerBlock * ntiles * int64_t(sizeof(int32_t))); }
-
-template <typename K>
-int allow_smem(K kernel, int bytes) {
-    if (bytes > 48 * 1024)
-        GSV_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-    return GSV_OK;
-}
+static_assert(kCsRowsPerBlock * kCsMaxTiles * 4 <= 48 * 1024, "counting-sort rows exceed 48 KB of shared memory");
 
 // Shared tail of both binning flavours.  Counting sort (k_colscan,
 // k_scatter) when the preprocess wrote the per-row tile counts (native path,
@@ -658,7 +654,6 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
             at<int32_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
         GSV_LAUNCH_CHECK();
         const int smem = cs_smem_bytes(T);
-        if (int rc = allow_smem(k_scatter, smem)) return rc;
         k_scatter<<<unsigned(prep_blocks(n)), 32 * kCsRowsPerBlock, smem, st>>>(
             at<int32_t>(ws_gauss, G.cs_pos), at<int4>(ws_gauss, G.box), offsets, n, T, rows, s, cap, vals_out, status,
             lb_cs, cs_col_blocks(T));
@@ -741,7 +736,6 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
     // status flags, the block counters and the scans' look-back words
     GSV_CUDA_TRY(cudaMemsetAsync(status, 0, status_bytes(n, si.ntiles), st));
     const int smem = L.cs ? cs_smem_bytes(si.ntiles) : 0;
-    if (int rc = allow_smem(k_prepare, smem)) return rc;
     k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, smem, st>>>(
         p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
         at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),

@@ -133,7 +133,7 @@ GSV_API int gsv_prepare_live(const gsv_params* params, const int32_t* live, gsv_
  * `capacity` pairs are kept and GSV_FLAG_CAPACITY_OVERFLOW is latched.  May
  * be called again after one preprocess (e.g. with a larger capacity).
  * Two sorts give the same lists: a counting sort over per-row tile counts
- * the preprocess writes when the grid has at most 4096 tiles and
+ * the preprocess writes when the grid has at most 3072 tiles and
  * ceil((n+1)/256)*4 rows x tiles <= 2^22 (three launches, no pair
  * keys), else an emit + radix sort + range pass.  gsv_bin picks the first
  * where it applies. */

@@ -144,7 +144,7 @@ def test_capacities_above_and_below_the_total(cuda_device):
 
 
 def test_counting_sort_refused_where_it_does_not_apply(cuda_device):
-    """More than 4096 tiles (the 256x256x160 volume has 20,480): the
+    """More than 3072 tiles (the 256x256x160 volume has 20,480): the
     counting mode is refused, the automatic mode takes the radix sort."""
     shape = (256, 256, 160)
     gs = synthetic.random_gaussians(2_000, shape, seed=1)
