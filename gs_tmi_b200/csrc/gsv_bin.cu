@@ -73,8 +73,8 @@ __host__ __device__ inline int64_t prep_blocks(int64_t n) { return (n + 1 + kPre
 // be repeated after one preprocess (e.g. with a larger capacity).
 constexpr int kCsSeg = 64;                                  // Gaussians per row: two warps of k_prepare
 constexpr int kCsRowsPerBlock = kPrepThreads / kCsSeg;      // rows per k_prepare block
-// k_prepare and k_scatter keep kCsRowsPerBlock x ntiles int32 in shared memory: at most 48 KB, the
-// size a launch may use without a function attribute (none is set, also not inside a graph capture)
+// k_scatter keeps kCsRowsPerBlock x ntiles int32 in shared memory: at most 48 KB, the size a
+// launch may use without a function attribute (none is set, also not inside a graph capture)
 constexpr int64_t kCsMaxTiles = 3072;
 constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles int32: 16 MB per matrix
 constexpr int kCsCols = 32, kCsRowGroups = 32;              // k_colscan block: 32 columns x 32 row groups
@@ -276,9 +276,10 @@ __device__ __forceinline__ int32_t box_tile(const DevShape& s, int bx, int by, i
 // only for its predecessors' published totals, each wait bounded (on
 // time-out GSV_FLAG_SCAN_STALLED is latched and the block publishes anyway,
 // so no later block waits the full limit again).  With `cs_mat` the block
-// also counts its pairs per tile for each of its kCsRowsPerBlock rows
-// (dynamic shared memory: kCsRowsPerBlock x ntiles int32) and writes those
-// rows of cs_mat.
+// also counts its pairs per tile for each of its kCsRowsPerBlock rows and
+// writes those rows of cs_mat.  A row's count in one tile is at most kCsSeg
+// (< 256), so the shared-memory counters are bytes, four to a word
+// (dynamic shared memory: kCsRowsPerBlock x ceil(ntiles/4) words).
 __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restrict__ pos,
                                                           const float* __restrict__ scl,
                                                           const float* __restrict__ rot,
@@ -364,15 +365,16 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
     // stride over the range and find each pair's Gaussian by a shuffle
     // search over the 32 starts (zero-count lanes share their successor's
     // start and are never chosen).
-    extern __shared__ int32_t cs_hist[];  // [kCsRowsPerBlock][ntiles]
-    for (int i = threadIdx.x; i < kCsRowsPerBlock * ntiles; i += kPrepThreads) cs_hist[i] = 0;
+    extern __shared__ uint32_t cs_hist[];  // [kCsRowsPerBlock][words]: byte counter of tile t in word t/4
+    const int words = (ntiles + 3) >> 2;
+    for (int i = threadIdx.x; i < kCsRowsPerBlock * words; i += kPrepThreads) cs_hist[i] = 0u;
     __syncthreads();
     {
         constexpr unsigned kAll = 0xffffffffu;
         const long long o = warp_base + incl - cnt;
         const long long wstart = __shfl_sync(kAll, o, 0);
         const long long wend = warp_base + warp_tot[warp];
-        int32_t* row = cs_hist + (warp * 32 / kCsSeg) * ntiles;
+        uint32_t* row = cs_hist + (warp * 32 / kCsSeg) * words;
         for (long long base = wstart; base < wend; base += 32) {
             const long long p = base + lane;
             int j = 0;  // largest j with o_j <= p
@@ -384,12 +386,17 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
             const long long oj = __shfl_sync(kAll, o, j);
             const int bx = __shfl_sync(kAll, box.x, j), by = __shfl_sync(kAll, box.y, j),
                       bz = __shfl_sync(kAll, box.z, j);
-            if (p < wend) atomicAdd(&row[box_tile(s, bx, by, bz, int32_t(p - oj))], 1);
+            if (p < wend) {
+                const int32_t t = box_tile(s, bx, by, bz, int32_t(p - oj));
+                atomicAdd(&row[t >> 2], 1u << ((t & 3) * 8));
+            }
         }
     }
     __syncthreads();
     int32_t* dst = cs_mat + bid * kCsRowsPerBlock * int64_t(ntiles);
-    for (int i = threadIdx.x; i < kCsRowsPerBlock * ntiles; i += kPrepThreads) dst[i] = cs_hist[i];
+    for (int r = 0; r < kCsRowsPerBlock; ++r)
+        for (int t = threadIdx.x; t < ntiles; t += kPrepThreads)
+            dst[r * ntiles + t] = int32_t((cs_hist[r * words + (t >> 2)] >> ((t & 3) * 8)) & 0xffu);
 }
 
 __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ center,
@@ -619,8 +626,13 @@ int sync_total(const GaussLayout& L, void* ws, int64_t n, int64_t* total_host, c
     return GSV_OK;
 }
 
-int cs_smem_bytes(int64_t ntiles) { return int(kCsRowsPerBlock * ntiles * int64_t(sizeof(int32_t))); }
-static_assert(kCsRowsPerBlock * kCsMaxTiles * 4 <= 48 * 1024, "counting-sort rows exceed 48 KB of shared memory");
+// Dynamic shared memory of k_prepare's byte counters and of k_scatter's positions.  Neither
+// kernel declares static shared memory beyond a few words, and both stay within the 48 KB a
+// launch may use without a function attribute.
+int cs_prep_smem_bytes(int64_t ntiles) { return int(kCsRowsPerBlock * ((ntiles + 3) / 4) * int64_t(sizeof(uint32_t))); }
+int cs_scatter_smem_bytes(int64_t ntiles) { return int(kCsRowsPerBlock * ntiles * int64_t(sizeof(int32_t))); }
+static_assert(kCsRowsPerBlock * kCsMaxTiles * 4 <= 48 * 1024, "k_scatter's positions exceed 48 KB");
+static_assert(kCsRowsPerBlock * kCsMaxTiles <= 40 * 1024, "k_prepare's counters leave no room for its static words");
 
 // Shared tail of both binning flavours.  Counting sort (k_colscan,
 // k_scatter) when the preprocess wrote the per-row tile counts (native path,
@@ -653,7 +665,7 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
         k_colscan<<<unsigned(cs_col_blocks(T)), kCsCols * kCsRowGroups, 0, st>>>(
             at<int32_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
         GSV_LAUNCH_CHECK();
-        const int smem = cs_smem_bytes(T);
+        const int smem = cs_scatter_smem_bytes(T);
         k_scatter<<<unsigned(prep_blocks(n)), 32 * kCsRowsPerBlock, smem, st>>>(
             at<int32_t>(ws_gauss, G.cs_pos), at<int4>(ws_gauss, G.box), offsets, n, T, rows, s, cap, vals_out, status,
             lb_cs, cs_col_blocks(T));
@@ -735,7 +747,7 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
     Status* status = at<Status>(ws_gauss, L.status);
     // status flags, the block counters and the scans' look-back words
     GSV_CUDA_TRY(cudaMemsetAsync(status, 0, status_bytes(n, si.ntiles), st));
-    const int smem = L.cs ? cs_smem_bytes(si.ntiles) : 0;
+    const int smem = L.cs ? cs_prep_smem_bytes(si.ntiles) : 0;
     k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, smem, st>>>(
         p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
         at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),
