@@ -145,29 +145,37 @@ def _time_to_target_eval(dev, n_train, n_eval, steps, mask_kind="poisson", repor
     torch.cuda.empty_cache()
     shape = (128, 128, 96)
     rows = []
+
+    def summary():
+        ratios = sorted(r["wall_ratio"] for r in rows if r.get("wall_ratio") is not None)
+        return {"mask": mask_kind, "train_phantoms": n_train, "eval_phantoms": n_eval, "train_steps": steps,
+                "seed_factor": wc.seed_factor, "seed_mode": wc.seed_mode, "loss": wc.loss,
+                "fit_lr_scale": wc.fit_lr_scale,
+                "train_examples": n_examples, "data_seconds": t_data,
+                "train_seconds": t_train, "first_train_loss": losses[0], "final_train_loss": losses[-1],
+                "evaluated": len(rows),
+                "median_wall_ratio": ratios[len(ratios) // 2] if ratios else None,
+                "reached": sum(r.get("warm_iterations_to_target") is not None for r in rows),
+                "warm_starts_lower": sum(r["warm_nmse_at_0"] < r["plain_nmse_at_0"] for r in rows),
+                "seeding_alone_reached": sum(r.get("seeded_iterations_to_target") is not None
+                                             for r in rows if "seeded_nmse_at_0" in r),
+                "eval": rows}
+
+    def write(report):
+        out = os.environ.get("GSV_REPORT_DIR")
+        if out and report_name:
+            os.makedirs(out, exist_ok=True)
+            with open(os.path.join(out, report_name), "w") as f:
+                json.dump(report, f, indent=1)
+
     for e in range(n_eval):
         case = synthetic.mri_case(shape, n_coils=8, accel=6.0, calib=24, seed=50_000 + e, mask_kind=mask_kind)
         rows.append(dict(warmstart.time_to_target(mlp, case, 50_000, seed=e, device=dev,
                                                   warm_points=int(round(50_000 * wc.seed_factor)),
                                                   warm_mode=wc.seed_mode, warm_schedule=wc.fit_overrides(),
                                                   ablation=e < ablations), phantom=e))
-    ratios = sorted(r["wall_ratio"] for r in rows if r.get("wall_ratio") is not None)
-    report = {"mask": mask_kind, "train_phantoms": n_train, "eval_phantoms": n_eval, "train_steps": steps,
-              "seed_factor": wc.seed_factor, "seed_mode": wc.seed_mode, "loss": wc.loss,
-              "fit_lr_scale": wc.fit_lr_scale,
-              "train_examples": n_examples, "data_seconds": t_data,
-              "train_seconds": t_train, "first_train_loss": losses[0], "final_train_loss": losses[-1],
-              "median_wall_ratio": ratios[len(ratios) // 2] if ratios else None,
-              "reached": sum(r.get("warm_iterations_to_target") is not None for r in rows),
-              "warm_starts_lower": sum(r["warm_nmse_at_0"] < r["plain_nmse_at_0"] for r in rows),
-              "seeding_alone_reached": sum(r.get("seeded_iterations_to_target") is not None
-                                           for r in rows if "seeded_nmse_at_0" in r),
-              "eval": rows}
-    out = os.environ.get("GSV_REPORT_DIR")
-    if out and report_name:
-        os.makedirs(out, exist_ok=True)
-        with open(os.path.join(out, report_name), "w") as f:
-            json.dump(report, f, indent=1)
+        write(summary())  # the report so far, after every acquisition
+    report = summary()
     print(json.dumps({k: v for k, v in report.items() if k != "eval"}), json.dumps(rows))
     return report
 
