@@ -269,7 +269,8 @@ __device__ __forceinline__ int32_t box_tile(const DevShape& s, int bx, int by, i
 }
 
 // Preprocess (center, radius, quadratic-form coefficients, tight extent, tile
-// box) of one Gaussian per thread, and the exclusive scan of the Gaussians'
+// box) of one Gaussian per thread, the clearing of its backward moment
+// accumulators, and the exclusive scan of the Gaussians'
 // pair counts into `offsets` (offsets[n] = pair total) in the same launch.
 // Blocks take their position in the scan from a counter in the status
 // region, so every block a block waits for has already started; it waits
@@ -289,7 +290,8 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
                                                           Rec* __restrict__ recs, float4* __restrict__ ext,
                                                           int4* __restrict__ boxes,
                                                           int64_t* __restrict__ offsets, Status* status,
-                                                          int32_t* __restrict__ cs_mat, int32_t ntiles) {
+                                                          int32_t* __restrict__ cs_mat, int32_t ntiles,
+                                                          float* __restrict__ accum) {
     __shared__ int bid_s;
     __shared__ int64_t warp_tot[kPrepThreads / 32];
     __shared__ int64_t block_base;
@@ -299,6 +301,10 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
     const int64_t g = bid * kPrepThreads + threadIdx.x;
     int64_t cnt = 0;
     int4 box = make_int4(0, 0, 0, 0);
+    if (g < n) {  // the backward's moment accumulators start from zero
+        float4* acc4 = reinterpret_cast<float4*>(accum + g * kMomStride);
+        acc4[0] = acc4[1] = acc4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     if (g < n && live && g >= int64_t(*live)) {  // parked row: no tiles, no contribution
         recs[g] = Rec{};
         ext[g] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -752,7 +758,7 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
         p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
         at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),
         at<int64_t>(ws_gauss, L.offsets), status, L.cs ? at<int32_t>(ws_gauss, L.cs_mat) : nullptr,
-        int32_t(si.ntiles));
+        int32_t(si.ntiles), at<float>(ws_gauss, L.accum));
     GSV_LAUNCH_CHECK();
     if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
     return GSV_OK;

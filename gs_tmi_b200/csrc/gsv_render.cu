@@ -992,13 +992,19 @@ __device__ __forceinline__ void gather_det_warp(const RenderArgs& a, int64_t g, 
     }
 }
 
-// Chain rule of one Gaussian from its 11 moments (accum).
+// Chain rule of one Gaussian from its 11 moments (accum).  The moments are
+// cleared once read: the preprocess clears them too, so the atomic backward
+// always starts from zero without a memset of its own.
 __device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
     const gsv_params& p = a.prm;
     const gsv_grads& out = a.grd;
     float mo[kMom];
 #pragma unroll
     for (int i = 0; i < kMom; ++i) mo[i] = a.accum[g * kMomStride + i];
+    {
+        float4* acc4 = reinterpret_cast<float4*>(a.accum + g * kMomStride);
+        acc4[0] = acc4[1] = acc4[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     const Rec R = a.recs[g];
     // dL/dcenter_vox, then dcenter/dpositions = 0.5 * shape = hs   (:284).
     // The reference sums this over included pairs only: a Gaussian with none
@@ -1358,9 +1364,9 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     a.offsets = cat<int64_t>(ws_gauss, G.offsets);
     a.boxes = cat<int4>(ws_gauss, G.box);
     a.capacity = capacity;
-    // deterministic: every listed pair's partial is written (zero where the
-    // pair adds nothing), so only the atomic accumulators need clearing
-    if (!det) GSV_CUDA_TRY(cudaMemsetAsync(a.accum, 0, size_t(n) * kMomStride * sizeof(float), st));
+    // The atomic accumulators are zero here: the preprocess clears them and
+    // k_finalize clears them again after reading.  The deterministic mode
+    // writes every listed pair's partial and its gather overwrites them.
     if (tuning) {
         a.chunk = tuning->chunk;
         a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);

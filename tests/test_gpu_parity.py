@@ -83,6 +83,27 @@ def test_deterministic_mode_is_bitwise_reproducible(cuda_device):
         assert np.array_equal(a.view(np.int32), b.view(np.int32))
 
 
+def test_repeated_backward_after_one_preprocess(cuda_device):
+    """The atomic backward's moment accumulators start from zero on every
+    call: the preprocess clears them and k_finalize clears them after
+    reading, so a second backward on the same binning gives the first's
+    gradients (to atomic-order rounding), not their sum."""
+    from gs_tmi_b200.tile_voxelizer import backward_into
+
+    shape, ts = (48, 40, 56), 8
+    gs = synthetic.random_gaussians(5000, shape, seed=21)
+    params = tuple(t.to(cuda_device).contiguous() for t in gs.tensors())
+    g = synthetic.upstream_grad(shape, seed=22).to(cuda_device)
+    plan = prepare_and_bin(params, _shape(shape, ts))
+    first = [torch.empty_like(t) for t in params]
+    second = [torch.empty_like(t) for t in params]
+    backward_into(plan, params, g, first)
+    backward_into(plan, params, g, second)
+    torch.cuda.synchronize()
+    for k, a, b in zip(GRAD_KEYS, first, second):
+        assert rel(b.cpu().numpy(), a.cpu().numpy()) < 1e-5, k
+
+
 def test_64cube_n20000(cuda_device):
     """The 64^3 / N=20,000 micro-benchmark workload at full size."""
     shape, ts = (64, 64, 64), 8
