@@ -268,6 +268,25 @@ __device__ __forceinline__ int32_t box_tile(const DevShape& s, int bx, int by, i
     return ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
 }
 
+// box_tile for the counting sort, where the pair index and both box extents
+// are below 4096 (they are at most the tile count, <= kCsMaxTiles): the two
+// integer divisions become trunc((x + 0.5) * rcp(n)) in IEEE single
+// precision, exact for 0 <= x < 4096 and 1 <= n <= 4096 (every pair checked
+// by enumeration), a few instructions instead of about twenty each.  r1, r2:
+// __frcp_rn of the box's n1, n2.
+__device__ __forceinline__ int32_t small_div(int32_t x, float rcp_n) {
+    return __float2int_rz(__fmul_rn(__fadd_rn(float(x), 0.5f), rcp_n));
+}
+__device__ __forceinline__ int32_t box_tile_small(const DevShape& s, int bx, int by, int bz, float r1, float r2,
+                                                  int32_t c) {
+    const int32_t t0 = bx & 0xffff, t1 = (bx >> 16) & 0xffff, t2 = by & 0xffff;
+    const int32_t n1 = bz & 0xffff, n2 = (bz >> 16) & 0xffff;
+    const int32_t r = small_div(c, r2), k = c - r * n2;
+    const int32_t i = small_div(r, r1), jj = r - i * n1;
+    return ((t0 + i) * s.nt[1] + (t1 + jj)) * s.nt[2] + (t2 + k);
+}
+__device__ __forceinline__ float box_rcp(int field) { return __frcp_rn(float(max(field & 0xffff, 1))); }
+
 // Preprocess (center, radius, quadratic-form coefficients, tight extent, tile
 // box) of one Gaussian per thread, the clearing of its backward moment
 // accumulators, and the exclusive scan of the Gaussians'
@@ -381,6 +400,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
         const long long wstart = __shfl_sync(kAll, o, 0);
         const long long wend = warp_base + warp_tot[warp];
         uint32_t* row = cs_hist + (warp * 32 / kCsSeg) * words;
+        const float rcp1 = box_rcp(box.z), rcp2 = box_rcp(box.z >> 16);
         for (long long base = wstart; base < wend; base += 32) {
             const long long p = base + lane;
             int j = 0;  // largest j with o_j <= p
@@ -392,8 +412,9 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
             const long long oj = __shfl_sync(kAll, o, j);
             const int bx = __shfl_sync(kAll, box.x, j), by = __shfl_sync(kAll, box.y, j),
                       bz = __shfl_sync(kAll, box.z, j);
+            const float r1 = __shfl_sync(kAll, rcp1, j), r2 = __shfl_sync(kAll, rcp2, j);
             if (p < wend) {
-                const int32_t t = box_tile(s, bx, by, bz, int32_t(p - oj));
+                const int32_t t = box_tile_small(s, bx, by, bz, r1, r2, int32_t(p - oj));
                 atomicAdd(&row[t >> 2], 1u << ((t & 3) * 8));
             }
         }
@@ -605,8 +626,9 @@ __global__ void __launch_bounds__(32 * kCsRowsPerBlock) k_scatter(const int32_t*
                       bz = __shfl_sync(kAll, mb.z, k);
             if (cnt <= 0) continue;  // warp-uniform
             const int32_t gid = int32_t(g0 + h + k);
+            const float r1 = box_rcp(bz), r2 = box_rcp(bz >> 16);
             for (int c = lane; c < cnt; c += 32) {
-                const int32_t t = box_tile(s, bx, by, bz, c);
+                const int32_t t = box_tile_small(s, bx, by, bz, r1, r2, c);
                 const int32_t p = at_t[t];
                 if (p < cap) pair_ids[p] = gid;
                 at_t[t] = int32_t(min(int64_t(p) + 1, cap));
