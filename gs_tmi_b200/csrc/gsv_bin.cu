@@ -63,7 +63,8 @@ __host__ __device__ inline int64_t prep_blocks(int64_t n) { return (n + 1 + kPre
 // final order is fixed by two facts: a tile's list holds its Gaussians in
 // ascending id, and Gaussians are handled in rows of kCsSeg consecutive ids.
 // k_prepare also writes, per row, how many of the row's pairs fall in each
-// tile (rows x tiles int32, "cs_mat"); k_colscan writes, per row and tile,
+// tile (rows x tiles bytes, "cs_mat": a row's count in one tile is at most
+// kCsSeg; rows padded to whole words); k_colscan writes, per row and tile,
 // the position of the row's first pair of that tile in the sorted output
 // ("cs_pos": the column's exclusive prefix plus the tile's start, from a
 // single-pass scan of the tile totals) and the tile ranges; k_scatter walks
@@ -80,6 +81,7 @@ constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles int3
 constexpr int kCsCols = 32, kCsRowGroups = 32;              // k_colscan block: 32 columns x 32 row groups
 __host__ __device__ inline int64_t cs_rows(int64_t n) { return prep_blocks(n) * kCsRowsPerBlock; }
 __host__ __device__ inline int64_t cs_col_blocks(int64_t ntiles) { return (ntiles + kCsCols - 1) / kCsCols; }
+__host__ __device__ inline int64_t cs_mstride(int64_t ntiles) { return (ntiles + 3) & ~int64_t(3); }  // bytes per row
 inline bool cs_eligible(int64_t n, int64_t ntiles) {
     return n > 0 && ntiles <= kCsMaxTiles && cs_rows(n) * ntiles <= kCsMaxCells;
 }
@@ -108,7 +110,7 @@ GaussLayout gauss_layout(int64_t n, const ShapeInfo& si) {
     L.accum = o;    o = align_up(o + size_t(n) * kMomStride * sizeof(float));
     L.status = o;   o = align_up(o + status_bytes(n, si.ntiles));
     L.cs = cs_eligible(n, si.ntiles);
-    L.cs_mat = o;   o = align_up(o + (L.cs ? size_t(cs_rows(n) * si.ntiles) * sizeof(int32_t) : 0));
+    L.cs_mat = o;   o = align_up(o + (L.cs ? size_t(cs_rows(n) * cs_mstride(si.ntiles)) : 0));
     L.cs_pos = o;   o = align_up(o + (L.cs ? size_t(cs_rows(n) * si.ntiles) * sizeof(int32_t) : 0));
     L.total = o;
     return L;
@@ -298,8 +300,9 @@ __device__ __forceinline__ float box_rcp(int field) { return __frcp_rn(float(max
 // so no later block waits the full limit again).  With `cs_mat` the block
 // also counts its pairs per tile for each of its kCsRowsPerBlock rows and
 // writes those rows of cs_mat.  A row's count in one tile is at most kCsSeg
-// (< 256), so the shared-memory counters are bytes, four to a word
-// (dynamic shared memory: kCsRowsPerBlock x ceil(ntiles/4) words).
+// (< 256), so the counters are bytes, four to a word, in shared memory
+// (dynamic: kCsRowsPerBlock x ceil(ntiles/4) words) and in cs_mat alike: the
+// block's rows go out as the same words.
 __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restrict__ pos,
                                                           const float* __restrict__ scl,
                                                           const float* __restrict__ rot,
@@ -309,7 +312,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
                                                           Rec* __restrict__ recs, float4* __restrict__ ext,
                                                           int4* __restrict__ boxes,
                                                           int64_t* __restrict__ offsets, Status* status,
-                                                          int32_t* __restrict__ cs_mat, int32_t ntiles,
+                                                          uint8_t* __restrict__ cs_mat, int32_t ntiles,
                                                           float* __restrict__ accum) {
     __shared__ int bid_s;
     __shared__ int64_t warp_tot[kPrepThreads / 32];
@@ -420,10 +423,9 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
         }
     }
     __syncthreads();
-    int32_t* dst = cs_mat + bid * kCsRowsPerBlock * int64_t(ntiles);
-    for (int r = 0; r < kCsRowsPerBlock; ++r)
-        for (int t = threadIdx.x; t < ntiles; t += kPrepThreads)
-            dst[r * ntiles + t] = int32_t((cs_hist[r * words + (t >> 2)] >> ((t & 3) * 8)) & 0xffu);
+    // tile t's byte is byte t of its row (little-endian words), so rows of words * 4 bytes
+    uint32_t* dst = reinterpret_cast<uint32_t*>(cs_mat + bid * kCsRowsPerBlock * cs_mstride(ntiles));
+    for (int i = threadIdx.x; i < kCsRowsPerBlock * words; i += kPrepThreads) dst[i] = cs_hist[i];
 }
 
 __global__ void __launch_bounds__(256) k_count_compat(const float* __restrict__ center,
@@ -528,7 +530,7 @@ __global__ void k_ranges(const int32_t* __restrict__ keys, const int64_t* __rest
 // tiles < t, from a single-pass look-back over the blocks' tile totals.
 // Writes every tile's range, (0,0) for an empty tile, clamped to `cap` (so a
 // truncated list never reaches past the pair buffer).
-__global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const int32_t* __restrict__ mat,
+__global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const uint8_t* __restrict__ mat,
                                                                     int32_t* __restrict__ pos, int64_t rows,
                                                                     int32_t ntiles, int64_t cap,
                                                                     int2* __restrict__ ranges, Status* status,
@@ -548,7 +550,7 @@ __global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const int32_
     int64_t sum = 0;
     if (col_ok) {
 #pragma unroll 8
-        for (int64_t r = r0; r < r1; ++r) sum += mat[r * ntiles + t];
+        for (int64_t r = r0; r < r1; ++r) sum += mat[r * cs_mstride(ntiles) + t];
     }
     part[rg][c] = sum;
     __syncthreads();
@@ -574,9 +576,8 @@ __global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const int32_
     if (!col_ok) return;
     int64_t at_r = start_s[c] + part[rg][c];
     for (int64_t r = r0; r < r1; ++r) {
-        const int64_t idx = r * ntiles + t;
-        pos[idx] = int32_t(min(at_r, cap));
-        at_r += mat[idx];
+        pos[r * ntiles + t] = int32_t(min(at_r, cap));
+        at_r += mat[r * cs_mstride(ntiles) + t];
     }
     if (rg == 0) {
         const int64_t st = start_s[c], tt = tot_s[c];
@@ -691,7 +692,7 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
         const int64_t rows = cs_rows(n);
         const int32_t T = int32_t(si.ntiles);
         k_colscan<<<unsigned(cs_col_blocks(T)), kCsCols * kCsRowGroups, 0, st>>>(
-            at<int32_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
+            at<uint8_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
         GSV_LAUNCH_CHECK();
         const int smem = cs_scatter_smem_bytes(T);
         k_scatter<<<unsigned(prep_blocks(n)), 32 * kCsRowsPerBlock, smem, st>>>(
@@ -779,7 +780,7 @@ static int prepare_impl(const gsv_params* p, const int32_t* live, gsv_shape shap
     k_prepare<<<unsigned(prep_blocks(n)), kPrepThreads, smem, st>>>(
         p->positions, p->scales, p->rotations, p->density_r, p->density_i, n, live, dev_shape(si),
         at<Rec>(ws_gauss, L.rec), at<float4>(ws_gauss, L.ext), at<int4>(ws_gauss, L.box),
-        at<int64_t>(ws_gauss, L.offsets), status, L.cs ? at<int32_t>(ws_gauss, L.cs_mat) : nullptr,
+        at<int64_t>(ws_gauss, L.offsets), status, L.cs ? at<uint8_t>(ws_gauss, L.cs_mat) : nullptr,
         int32_t(si.ntiles), at<float>(ws_gauss, L.accum));
     GSV_LAUNCH_CHECK();
     if (total_pairs_host) return sync_total(L, ws_gauss, n, total_pairs_host, st);
