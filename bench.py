@@ -196,8 +196,8 @@ def run_batched(args, rank, world, dist):
            "config": {"workload": "batch12", "volumes": [list(s) for s, _ in BATCH12],
                       "gaussians": [n for _, n in BATCH12], "tile_size": TILE, "evals_per_step": evals,
                       "autotuned_chunk_per_volume": chunks,
-                      "launch": "per-volume binning + 1 persistent forward + 1 persistent backward (+zero, "
-                                "finalize), one CUDA graph per iteration",
+                      "launch": "per-volume binning + 1 persistent forward + 1 persistent backward (+finalize), "
+                                "one CUDA graph per iteration",
                       "l2": "flushed between steps (256 MB write, untimed)", "parallelism": "replicas"},
            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                           "min": lat[0], "max": lat[-1]},

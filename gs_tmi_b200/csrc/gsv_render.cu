@@ -1148,18 +1148,6 @@ __global__ void __launch_bounds__(kThreads, 6) k_backward8_batched(const BatchTa
     }
 }
 
-// Zero the atomic accumulators of every volume (the deterministic backward
-// writes every listed pair's partial and needs no clearing).
-__global__ void k_zero_batched(const BatchTable t) {
-    const int64_t total = t.det ? 0 : t.gauss_prefix[t.count] * kMomStride;
-    for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
-         x += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t row = x / kMomStride;
-        const int i = find_item(t.gauss_prefix, t.count, row);
-        t.items[i].accum[x - t.gauss_prefix[i] * kMomStride] = 0.0f;
-    }
-}
-
 __global__ void __launch_bounds__(256) k_finalize_batched(const BatchTable t) {
     const int64_t total = t.gauss_prefix[t.count];
     for (int64_t x = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < total;
@@ -1606,9 +1594,9 @@ int gsv_backward_batched(void* ws_batch, int count, int flags, void* stream) {
     const bool det = flags & GSV_BACKWARD_DETERMINISTIC;
     BatchTable t = batch_table(ws_batch, count, det);
     GSV_CUDA_TRY(cudaMemsetAsync(t.counters, 0, 2 * sizeof(unsigned long long), st));
-    const int grid = persistent_grid(reinterpret_cast<const void*>(k_zero_batched), 256);
-    k_zero_batched<<<grid, 256, 0, st>>>(t);
-    GSV_LAUNCH_CHECK();
+    // every volume's accumulators are zero: its preprocess cleared them and
+    // k_finalize(_batched) clears them again after reading
+    const int grid = persistent_grid(reinterpret_cast<const void*>(k_finalize_batched), 256);
     if (det) k_backward8_batched<true><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<true>), kThreads), kThreads, 0, st>>>(t);
     else k_backward8_batched<false><<<persistent_grid(reinterpret_cast<const void*>(k_backward8_batched<false>), kThreads), kThreads, 0, st>>>(t);
     GSV_LAUNCH_CHECK();
