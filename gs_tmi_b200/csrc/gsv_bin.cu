@@ -317,7 +317,6 @@ __global__ void __launch_bounds__(kPrepThreads) k_prepare(const float* __restric
     __shared__ int bid_s;
     __shared__ int64_t warp_tot[kPrepThreads / 32];
     __shared__ int64_t block_base;
-    pdl_enter();  // launched after a memset: the wait returns at once; the successor may be scheduled early
     if (threadIdx.x == 0) bid_s = atomicAdd(&status->pad[1], 1);
     __syncthreads();
     const int64_t bid = bid_s;
@@ -539,7 +538,6 @@ __global__ void __launch_bounds__(kCsCols * kCsRowGroups) k_colscan(const uint8_
     __shared__ int bid_s;
     __shared__ int64_t part[kCsRowGroups][kCsCols];  // a row group's sum, then its exclusive prefix
     __shared__ int64_t start_s[kCsCols], tot_s[kCsCols];
-    pdl_enter();
     if (threadIdx.x == 0) bid_s = atomicAdd(&status->pad[2], 1);
     __syncthreads();
     const int64_t bid = bid_s;
@@ -604,7 +602,6 @@ __global__ void __launch_bounds__(32 * kCsRowsPerBlock) k_scatter(const int32_t*
                                                                   int64_t lb_words) {
     constexpr unsigned kAll = 0xffffffffu;
     extern __shared__ int32_t cs_at[];  // [kCsRowsPerBlock][ntiles]
-    pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (blockIdx.x == 0) {
         if (threadIdx.x == 0) {
@@ -694,13 +691,14 @@ int bin_common(const ShapeInfo& si, int64_t n, void* ws_gauss, void* ws_pairs, s
         unsigned long long* lb_cs = reinterpret_cast<unsigned long long*>(status + 1) + prep_blocks(n);
         const int64_t rows = cs_rows(n);
         const int32_t T = int32_t(si.ntiles);
-        GSV_CUDA_TRY(launch_pdl(k_colscan, dim3(unsigned(cs_col_blocks(T))), dim3(kCsCols * kCsRowGroups), 0, st,
-                                at<uint8_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap,
-                                ranges, status, lb_cs));
+        k_colscan<<<unsigned(cs_col_blocks(T)), kCsCols * kCsRowGroups, 0, st>>>(
+            at<uint8_t>(ws_gauss, G.cs_mat), at<int32_t>(ws_gauss, G.cs_pos), rows, T, cap, ranges, status, lb_cs);
+        GSV_LAUNCH_CHECK();
         const int smem = cs_scatter_smem_bytes(T);
-        GSV_CUDA_TRY(launch_pdl(k_scatter, dim3(unsigned(prep_blocks(n))), dim3(32 * kCsRowsPerBlock), size_t(smem), st,
-                                at<int32_t>(ws_gauss, G.cs_pos), at<int4>(ws_gauss, G.box), offsets, n, T, rows, s,
-                                cap, vals_out, status, lb_cs, cs_col_blocks(T)));
+        k_scatter<<<unsigned(prep_blocks(n)), 32 * kCsRowsPerBlock, smem, st>>>(
+            at<int32_t>(ws_gauss, G.cs_pos), at<int4>(ws_gauss, G.box), offsets, n, T, rows, s, cap, vals_out, status,
+            lb_cs, cs_col_blocks(T));
+        GSV_LAUNCH_CHECK();
         return GSV_OK;
     }
     // enough CTAs for the emission (one thread per Gaussian) and for the fills

@@ -135,35 +135,6 @@ __device__ __forceinline__ float4 tight_extent(const float qc[6]) {
                        __double2float_ru(sqrt(f * s2) + 0.01), 0.f);
 }
 
-// Programmatic dependent launch.  The kernels of one voxelizer step are
-// launched with cudaLaunchAttributeProgrammaticStreamSerialization, so a
-// kernel may be scheduled while its predecessor's last blocks still run.
-// Each such kernel first waits, before any global memory access, until the
-// predecessor grid has completed and its writes are visible (a no-op for a
-// kernel launched without the attribute), then lets its own successor be
-// scheduled.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
-// Launch `kernel` with the programmatic-serialization attribute (see pdl_enter).
-template <typename... KArgs, typename... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                              Args&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
-}
-
 // Row terms of the quadratic form for fixed (e0, e1):
 //   m(e2) = fma(fma(q22, e2, B), e2, A)
 __device__ __forceinline__ float row_a(const Rec& g, float e0, float e1) {

@@ -452,7 +452,6 @@ template <bool COMPAT, bool PLANAR, int RPL>
 __global__ void __launch_bounds__(kThreads) k_forward8(const RenderArgs a) {
     __shared__ __align__(16) unsigned char smem_raw[kFwdSmem];
     constexpr int subs = 2 / RPL;
-    pdl_enter();
     forward_tile<COMPAT, PLANAR, RPL>(a, blockIdx.x / subs, blockIdx.x % subs, smem_raw);
 }
 
@@ -613,7 +612,6 @@ template <bool COMPAT, bool DET, int RPL>
 __global__ void __launch_bounds__(kThreads, RPL == 2 ? 6 : 7) k_backward8(const RenderArgs a) {
     __shared__ __align__(16) WarpStage stage[kWarps];
     constexpr int subs = 2 / RPL;
-    pdl_enter();
     const int part = blockIdx.x % a.split, rest = blockIdx.x / a.split;
     backward_tile<COMPAT, DET, RPL>(a, rest / subs, rest % subs, stage, part);
 }
@@ -1080,7 +1078,6 @@ __device__ __forceinline__ void finalize_one(const RenderArgs& a, int64_t g) {
 }
 
 __global__ void __launch_bounds__(256) k_finalize(const RenderArgs a) {
-    pdl_enter();
     const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= a.prm.n) return;
     finalize_one(a, g);
@@ -1088,7 +1085,6 @@ __global__ void __launch_bounds__(256) k_finalize(const RenderArgs a) {
 
 // One warp per Gaussian (deterministic backward).
 __global__ void __launch_bounds__(256) k_gather_det(const RenderArgs a) {
-    pdl_enter();
     const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     if (g >= a.prm.n) return;  // warp-uniform
     gather_det_warp(a, g, threadIdx.x & 31);
@@ -1312,10 +1308,8 @@ int gsv_forward_ex(gsv_shape shape, int64_t n, const void* ws_gauss, const void*
         a.chunk = tuning->chunk;
         a.cull = !(tuning->flags & GSV_TUNE_NO_CULL);
     }
-    if (shape.tile_size == 8 && rpl == 2)
-        GSV_CUDA_TRY(launch_pdl(k_forward8<false, false, 2>, dim3(unsigned(ntiles)), dim3(kThreads), 0, st, a));
-    else if (shape.tile_size == 8)
-        GSV_CUDA_TRY(launch_pdl(k_forward8<false, false, 1>, dim3(unsigned(2 * ntiles)), dim3(kThreads), 0, st, a));
+    if (shape.tile_size == 8 && rpl == 2) k_forward8<false, false, 2><<<unsigned(ntiles), kThreads, 0, st>>>(a);
+    else if (shape.tile_size == 8) k_forward8<false, false, 1><<<unsigned(2 * ntiles), kThreads, 0, st>>>(a);
     else if (shape.tile_size == 4)
         k_forward4<false, false><<<unsigned((ntiles + kWarps - 1) / kWarps), kThreads, 0, st>>>(a);
     else k_forward_generic<false, false><<<unsigned(ntiles), kThreads, 0, st>>>(a);
@@ -1371,15 +1365,9 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     const unsigned sp = unsigned(a.split);
     if (capacity > 0) {
         if (shape.tile_size == 8) {
-            if (det)
-                GSV_CUDA_TRY(launch_pdl(k_backward8<false, true, 2>, dim3(unsigned(ntiles) * sp), dim3(kThreads), 0,
-                                        st, a));
-            else if (rpl == 2)
-                GSV_CUDA_TRY(launch_pdl(k_backward8<false, false, 2>, dim3(unsigned(ntiles) * sp), dim3(kThreads), 0,
-                                        st, a));
-            else
-                GSV_CUDA_TRY(launch_pdl(k_backward8<false, false, 1>, dim3(unsigned(2 * ntiles) * sp),
-                                        dim3(kThreads), 0, st, a));
+            if (det) k_backward8<false, true, 2><<<unsigned(ntiles) * sp, kThreads, 0, st>>>(a);
+            else if (rpl == 2) k_backward8<false, false, 2><<<unsigned(ntiles) * sp, kThreads, 0, st>>>(a);
+            else k_backward8<false, false, 1><<<unsigned(2 * ntiles) * sp, kThreads, 0, st>>>(a);
         } else {
             const unsigned g4 = unsigned((ntiles + kWarps - 1) / kWarps);
             if (shape.tile_size == 4 && det) k_backward4<false, true><<<g4, kThreads, 0, st>>>(a);
@@ -1392,10 +1380,10 @@ int gsv_backward_ex(const gsv_params* p, gsv_shape shape, void* ws_gauss, void* 
     a.prm = *p;
     a.grd = *grads;
     if (det) {
-        GSV_CUDA_TRY(launch_pdl(k_gather_det, dim3(grid_for(n * 32, 256)), dim3(256), 0, st, a));
+        k_gather_det<<<grid_for(n * 32, 256), 256, 0, st>>>(a);
         GSV_LAUNCH_CHECK();
     }
-    GSV_CUDA_TRY(launch_pdl(k_finalize, dim3(grid_for(n, 256)), dim3(256), 0, st, a));
+    k_finalize<<<grid_for(n, 256), 256, 0, st>>>(a);
     GSV_LAUNCH_CHECK();
     return GSV_OK;
 }
