@@ -77,7 +77,7 @@ constexpr int kCsRowsPerBlock = kPrepThreads / kCsSeg;      // rows per k_prepar
 // k_scatter keeps kCsRowsPerBlock x ntiles int32 in shared memory: at most 48 KB, the size a
 // launch may use without a function attribute (none is set, also not inside a graph capture)
 constexpr int64_t kCsMaxTiles = 3072;
-constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles int32: 16 MB per matrix
+constexpr int64_t kCsMaxCells = int64_t(1) << 22;           // rows x tiles: 4 MB of counts, 16 MB of positions
 constexpr int kCsCols = 32, kCsRowGroups = 32;              // k_colscan block: 32 columns x 32 row groups
 __host__ __device__ inline int64_t cs_rows(int64_t n) { return prep_blocks(n) * kCsRowsPerBlock; }
 __host__ __device__ inline int64_t cs_col_blocks(int64_t ntiles) { return (ntiles + kCsCols - 1) / kCsCols; }
